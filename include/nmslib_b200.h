@@ -1,0 +1,122 @@
+/*
+ * nmslib_b200 — C ABI of the B200 (sm_100a) engine for NMSLIB's HNSW query path.
+ *
+ * Plain pointers and sizes only. Each entry point replaces one piece of the reference's
+ * Python-facing interface (paths are relative to the reference project root):
+ *
+ *   nmsg_index_load        IndexWrapper::loadIndex        python_bindings/nmslib.cc:98-113
+ *                          -> Hnsw::LoadIndex / LoadOptimizedIndex  similarity_search/src/method/hnsw.cc:993-1074
+ *   nmsg_set_query_params  setQueryTimeParams lambda      python_bindings/nmslib.cc:599-607
+ *                          -> Hnsw::SetQueryTimeParams    similarity_search/src/method/hnsw.cc:472-507
+ *   nmsg_knn_batch         IndexWrapper::knnQueryBatch    python_bindings/nmslib.cc:142-168
+ *                          -> Hnsw::Search(KNNQuery*)     similarity_search/src/method/hnsw.cc:717-746
+ *                          -> SearchV1Merge / SearchOld   similarity_search/src/method/hnsw_distfunc_opt.cc:46-283
+ *   nmsg_knn_batch (nq=1)  IndexWrapper::knnQuery         python_bindings/nmslib.cc:127-140
+ *   nmsg_index_save        IndexWrapper::saveIndex        python_bindings/nmslib.cc:115-125
+ *                          -> Hnsw::SaveOptimizedIndex    similarity_search/src/method/hnsw.cc:774-806
+ *   nmsg_index_free        IndexWrapper destructor (index.reset)
+ *   nmsg_last_error        the message of the C++ exception the reference would throw
+ *                          (CHECK_MSG / runtime_error, similarity_search/include/logging.h:123-135)
+ *
+ * Every call returns NMSG_OK (0) or a negative status; nmsg_last_error() then holds a message
+ * (thread-local). Kernels never trap: device-side failures are written to a status word and
+ * reported as a status here.
+ */
+#ifndef NMSLIB_B200_H_
+#define NMSLIB_B200_H_
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NMSG_API __attribute__((visibility("default")))
+#else
+#define NMSG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nmsg_index nmsg_index;
+
+enum nmsg_status {
+  NMSG_OK = 0,
+  NMSG_ERR_BAD_FILE = -1,      /* missing, truncated or malformed index file */
+  NMSG_ERR_UNSUPPORTED = -2,   /* e.g. a non-optimized (regular) index, or L1/LInf codes */
+  NMSG_ERR_BAD_ARG = -3,       /* argument out of range, dimension mismatch, ... */
+  NMSG_ERR_OOM = -4,           /* device or pinned-host allocation failed */
+  NMSG_ERR_DEVICE = -5,        /* CUDA runtime error */
+  NMSG_ERR_TIMEOUT = -6,       /* a bounded device wait gave up */
+  NMSG_ERR_CORRUPT_GRAPH = -7, /* neighbour id out of range, count above maxM/maxM0, ... */
+  NMSG_ERR_CAPACITY = -8       /* a per-query device buffer would overflow */
+};
+
+/* Space names of nmslib.init(space=...): 'l2', 'cosinesimil', 'negdotprod'. */
+enum nmsg_space { NMSG_SPACE_L2 = 0, NMSG_SPACE_COSINE = 1, NMSG_SPACE_NEGDOT = 2 };
+
+/* algoType of setQueryTimeParams (hnsw.cc:486-497): hybrid uses SearchOld when ef >= 1000. */
+enum nmsg_algo { NMSG_ALGO_HYBRID = 0, NMSG_ALGO_OLD = 1, NMSG_ALGO_V1MERGE = 2 };
+
+/* nmsg_knn_batch flags */
+enum nmsg_flags {
+  NMSG_DEVICE_PTRS = 1, /* queries and outputs are device pointers; no host copies, no sync */
+  NMSG_PLAIN_KERNEL = 2 /* one query per CUDA block (the unbatched kernel) instead of the
+                           persistent work-queue kernel */
+};
+
+typedef struct nmsg_index_info {
+  int64_t n;            /* stored elements (totalElementsStored_) */
+  int32_t dim;          /* vector length */
+  int32_t dist_type;    /* DistFuncType code from the file: 1 L2Sqr16Ext, 2 L2SqrExt,
+                           3 NormCosine, 4 NegativeDotProduct (hnsw.h:50-58) */
+  int32_t maxlevel;
+  int32_t enterpoint;
+  int32_t maxM;
+  int32_t maxM0;
+  int32_t ef;           /* current query-time ef (20 after load, hnsw.cc:483) */
+  int32_t algo;         /* current nmsg_algo */
+  int32_t device;
+  int64_t device_bytes; /* resident index bytes on the device */
+} nmsg_index_info;
+
+/* Load an optimized HNSW index file (the output of the reference's saveIndex) onto `device`.
+ * `space` must agree with the file's distance code. ef is reset to 20 and algo to hybrid,
+ * as IndexWrapper::loadIndex does through ResetQueryTimeParams (nmslib.cc:112). */
+NMSG_API int nmsg_index_load(const char* path, int space, int device, nmsg_index** out);
+
+/* Write the loaded index back in the reference's optimized format (hnsw.cc:774-806). */
+NMSG_API int nmsg_index_save(const nmsg_index* index, const char* path);
+
+NMSG_API void nmsg_index_free(nmsg_index* index);
+
+NMSG_API int nmsg_index_info_get(const nmsg_index* index, nmsg_index_info* out);
+
+/* efSearch (>= 1) and algoType; applied to later nmsg_knn_batch calls. */
+NMSG_API int nmsg_set_query_params(nmsg_index* index, int ef, int algo);
+
+/* k-NN for nq queries of length dim (row-major float32).
+ *   k_per_q / ef_per_q: optional per-query k and ef (NULL -> `k` / the index's ef).
+ *   kmax: row stride of ids/dists (>= every k used).
+ *   ids   [nq * kmax]: external ids (the ids stored in each node's object header), -1 padding.
+ *   dists [nq * kmax]: distances in ascending order, +inf padding. l2 reports SQUARED
+ *                      distance, as the reference's optimized path does.
+ *   counts[nq]: results per query, min(k, found).
+ *   stats [nq * 4] (optional): distance evaluations, level-0 expansions, upper-level list
+ *                      scans, algorithmic bytes read.
+ *   stream: a cudaStream_t (NULL = the legacy default stream).
+ * Host pointers (default): copies in and out, synchronous. NMSG_DEVICE_PTRS: device pointers,
+ * asynchronous on `stream`. Calls on one handle are serialised. */
+NMSG_API int nmsg_knn_batch(nmsg_index* index, const float* queries, int64_t nq, int32_t dim, int32_t k,
+                   const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids,
+                   float* dists, int32_t* counts, int64_t* stats, uint32_t flags, void* stream);
+
+/* Device status of the last batch on this handle (NMSG_OK or a device-side error code). */
+NMSG_API int nmsg_last_device_status(const nmsg_index* index);
+
+NMSG_API const char* nmsg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NMSLIB_B200_H_ */

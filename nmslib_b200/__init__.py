@@ -1,0 +1,219 @@
+"""nmslib_b200 — a B200 (sm_100a) engine behind NMSLIB's Python surface for the HNSW query path.
+
+Drop-in for the reference's ``nmslib`` module on this path::
+
+    import nmslib_b200 as nmslib
+    index = nmslib.init(method='hnsw', space='l2')        # 'l2' | 'cosinesimil' | 'negdotprod'
+    index.loadIndex('index.hnsw')                          # a file written by the reference's saveIndex
+    index.setQueryTimeParams({'efSearch': 100})
+    results = index.knnQueryBatch(queries, k=10)           # [(ids int32[], dists float32[]), ...]
+
+Names, argument meaning and error behaviour follow python_bindings/nmslib.cc (``init`` :470-510,
+``IndexWrapper`` :67-376, ``loadParams`` :658-692). The search itself runs in the CUDA engine
+(include/nmslib_b200.h); there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+
+import numpy as np
+
+from . import _capi
+
+__version__ = "0.1.0"
+
+SPACES = {"l2": _capi.SPACE_L2, "cosinesimil": _capi.SPACE_COSINE, "negdotprod": _capi.SPACE_NEGDOT}
+METHODS = ("hnsw",)
+_ALGOS = {"hybrid": _capi.ALGO_HYBRID, "old": _capi.ALGO_OLD, "v1merge": _capi.ALGO_V1MERGE}
+
+
+class DistType(enum.IntEnum):
+    FLOAT = 0
+    INT = 1
+
+
+class DataType(enum.IntEnum):
+    DENSE_VECTOR = 0
+    DENSE_UINT8_VECTOR = 1
+    SPARSE_VECTOR = 2
+    OBJECT_AS_STRING = 3
+
+
+def _load_params(o):
+    """dict or ['key=value', ...] -> {key: str}; python_bindings/nmslib.cc:658-692."""
+    if o is None:
+        return {}
+    if isinstance(o, list):
+        out = {}
+        for item in o:
+            if not isinstance(item, str) or "=" not in item:
+                raise ValueError(f"Wrong format of the parameter string: {item!r}")
+            key, val = item.split("=", 1)
+            out[key.strip()] = val.strip()
+        return out
+    if isinstance(o, dict):
+        out = {}
+        for key, val in o.items():
+            if isinstance(val, bool) or not isinstance(val, (int, float, str)):
+                raise ValueError(f"Unknown type for parameter '{key}'")
+            out[str(key)] = str(int(val)) if isinstance(val, float) and float(val).is_integer() else str(val)
+        return out
+    raise ValueError("Unknown type for parameters")
+
+
+def _as_int(key, val):
+    try:
+        return int(val)
+    except ValueError:
+        raise RuntimeError(f"Failed to convert value '{val}' of parameter '{key}' to an integer") from None
+
+
+class FloatIndex:
+    """Mirror of ``IndexWrapper<float>`` for method='hnsw' over dense float vectors."""
+
+    def __init__(self, method, space, space_params, data_type, dtype, device=0):
+        if method not in METHODS:
+            raise ValueError(f"The B200 engine implements method 'hnsw' only, got {method!r}")
+        if space not in SPACES:
+            raise ValueError(f"The B200 engine implements spaces {sorted(SPACES)}, got {space!r}")
+        if _load_params(space_params):
+            raise RuntimeError("Unknown parameters found!")
+        if data_type != DataType.DENSE_VECTOR:
+            raise ValueError(f"The space type {space} is not compatible with the type {DataType(data_type).name}, "
+                             "only dense vector spaces are allowed!")
+        if dtype != DistType.FLOAT:
+            raise ValueError("The B200 engine implements DistType.FLOAT only")
+        self.method, self.space, self.device = method, space, int(device)
+        self.dataType, self.distType = DataType(data_type), DistType(dtype)
+        self._h = ctypes.c_void_p()
+        self._info = None
+
+    # ------------------------------------------------------------------ lifecycle
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _capi._lib is not None:
+            _capi._lib.nmsg_index_free(h)
+            self._h = ctypes.c_void_p()
+
+    def _require(self):
+        if not self._h:
+            raise ValueError("Must call createIndex or loadIndex before this method")
+        return self._h
+
+    def loadIndex(self, filename, load_data=False):
+        """IndexWrapper::loadIndex (nmslib.cc:98-113): reads the optimized index file and resets
+        the query-time parameters (ef = 20, algoType = hybrid)."""
+        if load_data:
+            raise ValueError("load_data=True is not supported: the optimized index file already holds the vectors")
+        lib = _capi.load()
+        h = ctypes.c_void_p()
+        _capi.check(lib.nmsg_index_load(os.fsencode(filename), SPACES[self.space], self.device, ctypes.byref(h)))
+        if self._h:
+            lib.nmsg_index_free(self._h)
+        self._h = h
+        self._refresh_info()
+
+    def saveIndex(self, filename, save_data=False):
+        if save_data:
+            raise ValueError("save_data=True is not supported by the B200 engine")
+        _capi.check(_capi.load().nmsg_index_save(self._require(), os.fsencode(filename)))
+
+    def _refresh_info(self):
+        info = _capi.IndexInfo()
+        _capi.check(_capi.load().nmsg_index_info_get(self._h, ctypes.byref(info)))
+        self._info = info
+
+    @property
+    def info(self) -> dict:
+        self._require()
+        self._refresh_info()
+        return {name: getattr(self._info, name) for name, _ in _capi.IndexInfo._fields_}
+
+    def __len__(self):
+        return int(self._info.n) if self._h else 0
+
+    def __repr__(self):
+        return f"<nmslib_b200.FloatIndex method={self.method} space={self.space} n={len(self)}>"
+
+    # ------------------------------------------------------------------ parameters
+    def setQueryTimeParams(self, params=None):
+        """Hnsw::SetQueryTimeParams (hnsw.cc:472-507): keys ef | efSearch (default 20),
+        algoType old | v1merge | hybrid (default hybrid), searchMethod (accepted, ignored).
+        Keys left out return to their defaults."""
+        h = self._require()
+        p = _load_params(params)
+        if "ef" in p and "efSearch" in p:
+            raise RuntimeError("The user shouldn't specify parameters ef and efSearch at the same time "
+                               "(they are synonyms)")
+        unknown = set(p) - {"ef", "efSearch", "algoType", "searchMethod"}
+        if unknown:
+            raise RuntimeError("Unknown parameters found!")
+        ef = _as_int("ef", p.get("ef", p.get("efSearch", "20")))
+        algo = p.get("algoType", "hybrid").lower()
+        if algo not in _ALGOS:
+            raise RuntimeError("algoType should be one of the following: old, v1merge")
+        if "searchMethod" in p:
+            _as_int("searchMethod", p["searchMethod"])
+        _capi.check(_capi.load().nmsg_set_query_params(h, ef, _ALGOS[algo]))
+
+    # ------------------------------------------------------------------ search
+    def _queries(self, input):
+        if isinstance(input, list):
+            rows = [np.ascontiguousarray(np.asarray(r, dtype=np.float32).reshape(-1)) for r in input]
+            if not rows:
+                return np.zeros((0, self._info.dim if self._info else 0), np.float32)
+            return np.ascontiguousarray(np.stack(rows))
+        q = np.ascontiguousarray(np.asarray(input, dtype=np.float32))
+        if q.ndim != 2:
+            raise RuntimeError("data must be a 2d array")
+        return q
+
+    def knnQueryBatchArrays(self, queries, k=10, ef=None, plain=False, stats=False):
+        """Batch search returning dense arrays: (ids [nq, kmax] int32 with -1 padding,
+        dists [nq, kmax] float32 with +inf padding, counts [nq] int32[, stats [nq, 4] int64]).
+        ``k`` and ``ef`` may be per-query integer arrays (mixed batches in one launch)."""
+        h = self._require()
+        q = self._queries(queries)
+        nq = q.shape[0]
+        k_arr = None
+        if np.ndim(k):
+            k_arr = np.ascontiguousarray(np.asarray(k, dtype=np.int32).reshape(-1))
+            if k_arr.shape[0] != nq:
+                raise ValueError("per-query k must have one entry per query")
+            kmax = int(k_arr.max()) if nq else 1
+        else:
+            kmax = int(k)
+        ef_arr = None
+        if ef is not None:
+            ef_arr = np.ascontiguousarray(np.broadcast_to(np.asarray(ef, dtype=np.int32), (nq,)))
+        kmax = max(kmax, 1)
+        ids = np.empty((nq, kmax), np.int32)
+        dists = np.empty((nq, kmax), np.float32)
+        counts = np.empty(nq, np.int32)
+        st = np.empty((nq, 4), np.int64) if stats else None
+        ptr = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        flags = _capi.FLAG_PLAIN_KERNEL if plain else 0
+        dim = q.shape[1] if nq else (self._info.dim if self._info else 0)
+        _capi.check(_capi.load().nmsg_knn_batch(h, ptr(q), nq, dim, 1 if k_arr is not None else kmax, ptr(k_arr),
+                                                ptr(ef_arr), kmax, ptr(ids), ptr(dists), ptr(counts), ptr(st),
+                                                flags, None))
+        return (ids, dists, counts, st) if stats else (ids, dists, counts)
+
+    def knnQueryBatch(self, queries, k=10, num_threads=0):
+        """IndexWrapper::knnQueryBatch (nmslib.cc:142-168): a list of (ids int32[], dists float32[])
+        per query, ascending distance. num_threads is accepted for compatibility and unused."""
+        ids, dists, counts = self.knnQueryBatchArrays(queries, k)
+        return [(ids[i, :c].copy(), dists[i, :c].copy()) for i, c in enumerate(counts.tolist())]
+
+    def knnQuery(self, vector, k=10):
+        """IndexWrapper::knnQuery (nmslib.cc:127-140)."""
+        v = np.asarray(vector, dtype=np.float32).reshape(1, -1)
+        return self.knnQueryBatch(v, k)[0]
+
+
+def init(space="cosinesimil", space_params=None, method="hnsw", data_type=DataType.DENSE_VECTOR,
+         dtype=DistType.FLOAT, device=0):
+    """nmslib.init (python_bindings/nmslib.cc:470-510); ``device`` selects the CUDA device."""
+    return FloatIndex(method, space, space_params, data_type, dtype, device)

@@ -1,0 +1,85 @@
+"""ctypes binding of the engine's C ABI (include/nmslib_b200.h).
+
+The shared library is built in-tree (nmslib_b200/libnmslib_b200.so, see build.py). There is no
+fallback: if the library is missing or cannot load, every search raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnmslib_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "nmslib_b200.h")
+
+OK = 0
+ERR_BAD_FILE, ERR_UNSUPPORTED, ERR_BAD_ARG, ERR_OOM = -1, -2, -3, -4
+ERR_DEVICE, ERR_TIMEOUT, ERR_CORRUPT_GRAPH, ERR_CAPACITY = -5, -6, -7, -8
+
+SPACE_L2, SPACE_COSINE, SPACE_NEGDOT = 0, 1, 2
+ALGO_HYBRID, ALGO_OLD, ALGO_V1MERGE = 0, 1, 2
+FLAG_DEVICE_PTRS, FLAG_PLAIN_KERNEL = 1, 2
+
+
+class IndexInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("dim", ctypes.c_int32), ("dist_type", ctypes.c_int32),
+                ("maxlevel", ctypes.c_int32), ("enterpoint", ctypes.c_int32), ("maxM", ctypes.c_int32),
+                ("maxM0", ctypes.c_int32), ("ef", ctypes.c_int32), ("algo", ctypes.c_int32),
+                ("device", ctypes.c_int32), ("device_bytes", ctypes.c_int64)]
+
+
+_lib = None
+
+
+def header_symbols():
+    """Names of every function the C header declares."""
+    with open(HEADER) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"NMSG_API\s+[\w\s\*]+?\b(nmsg_\w+)\s*\(", text)))
+
+
+def load(path: str = LIB_PATH):
+    """Load the engine library (once) and declare argument types."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"nmslib_b200 engine library not built ({path}); run `python -m nmslib_b200.build`")
+    lib = ctypes.CDLL(path)
+    P, I32, I64, U32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32
+    lib.nmsg_index_load.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
+    lib.nmsg_index_load.restype = ctypes.c_int
+    lib.nmsg_index_save.argtypes = [P, ctypes.c_char_p]
+    lib.nmsg_index_save.restype = ctypes.c_int
+    lib.nmsg_index_free.argtypes = [P]
+    lib.nmsg_index_free.restype = None
+    lib.nmsg_index_info_get.argtypes = [P, ctypes.POINTER(IndexInfo)]
+    lib.nmsg_index_info_get.restype = ctypes.c_int
+    lib.nmsg_set_query_params.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    lib.nmsg_set_query_params.restype = ctypes.c_int
+    lib.nmsg_knn_batch.argtypes = [P, P, I64, I32, I32, P, P, I32, P, P, P, P, U32, P]
+    lib.nmsg_knn_batch.restype = ctypes.c_int
+    lib.nmsg_last_device_status.argtypes = [P]
+    lib.nmsg_last_device_status.restype = ctypes.c_int
+    lib.nmsg_last_error.argtypes = []
+    lib.nmsg_last_error.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().nmsg_last_error().decode(errors="replace")
+
+
+def check(rc: int):
+    """Map a status to the exception type the reference raises for the same failure
+    (std::invalid_argument -> ValueError, runtime_error -> RuntimeError)."""
+    if rc == OK:
+        return
+    msg = last_error()
+    if rc == ERR_BAD_ARG:
+        raise ValueError(msg)
+    if rc == ERR_OOM:
+        raise MemoryError(msg)
+    raise RuntimeError(msg)

@@ -1,0 +1,408 @@
+// C ABI of the engine (declared in include/nmslib_b200.h): index upload, query-time parameters,
+// batch search with host or device buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "../../include/nmslib_b200.h"
+
+using namespace nmsg;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? NMSG_ERR_OOM : NMSG_ERR_DEVICE;
+}
+
+#define NMSG_CUDA(call, what)                      \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// A grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t want, bool zero) {
+    if (want <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) return e;
+    bytes = want;
+    if (zero) return cudaMemset(p, 0, want);
+    return cudaSuccess;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kMaxSmemPerBlock = 227 * 1024;
+
+}  // namespace
+
+struct nmsg_index {
+  int device = 0;
+  int space = 0;
+  int ef = 20;
+  int algo = NMSG_ALGO_HYBRID;
+  int num_sms = 0;
+  HostIndex host;
+  DevIndex dev;
+  DevBuf vecs, l0, up_off, up_links, ext_id;
+  // search scratch (grown on demand)
+  DevBuf visited, epochs, locks, old_heap, counter, status, order, kq, efq;
+  DevBuf q_stage, ids_stage, dists_stage, counts_stage, stats_stage;
+  int slots = 0;            // slots covered by visited/epochs/locks
+  int64_t old_cap = 0;      // entries per slot in old_heap
+  int64_t resident_bytes = 0;
+  int last_status = NMSG_OK;
+  std::mutex mu;
+};
+
+namespace {
+
+int upload_index(nmsg_index* h) {
+  const HostIndex& hi = h->host;
+  DevIndex& d = h->dev;
+  d = DevIndex();
+  d.n = hi.n;
+  if (hi.n == 0) return NMSG_OK;
+  d.dim = hi.dim;
+  d.pitch = (hi.dim + 31) & ~31;
+  d.n16 = hi.dim & ~15;
+  d.n4 = hi.dim & ~3;
+  d.maxM = (int)hi.maxM;
+  d.maxM0 = (int)hi.maxM0;
+  d.l0_pitch = ((int)hi.maxM0 + 1 + 7) & ~7;
+  d.maxlevel = hi.maxlevel;
+  d.enterpoint = (int)hi.enterpoint;
+  d.dist_type = hi.dist_type;
+
+  const int64_t n = hi.n;
+  std::vector<float> vec((size_t)n * d.pitch, 0.0f);
+  std::vector<int32_t> l0((size_t)n * d.l0_pitch, 0);
+  std::vector<int32_t> ext(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const float* src = hi.vec(i);
+    float* dst = vec.data() + i * d.pitch;
+    for (int e = 0; e < hi.dim; ++e) dst[permuted_pos(e, hi.dim)] = src[e];
+    const int32_t* lst = hi.l0(i);
+    std::memcpy(l0.data() + i * d.l0_pitch, lst, 4 * (1 + lst[0]));
+    ext[i] = hi.ext_id(i);
+  }
+  std::vector<int32_t> links = hi.up_links;
+  if (links.empty()) links.push_back(0);
+  NMSG_CUDA(h->vecs.ensure(vec.size() * 4, false), "cudaMalloc(vectors)");
+  NMSG_CUDA(h->l0.ensure(l0.size() * 4, false), "cudaMalloc(level-0 lists)");
+  NMSG_CUDA(h->up_off.ensure(n * 8, false), "cudaMalloc(upper offsets)");
+  NMSG_CUDA(h->up_links.ensure(links.size() * 4, false), "cudaMalloc(upper lists)");
+  NMSG_CUDA(h->ext_id.ensure(n * 4, false), "cudaMalloc(ids)");
+  NMSG_CUDA(cudaMemcpy(h->vecs.p, vec.data(), vec.size() * 4, cudaMemcpyHostToDevice), "upload vectors");
+  NMSG_CUDA(cudaMemcpy(h->l0.p, l0.data(), l0.size() * 4, cudaMemcpyHostToDevice), "upload lists");
+  NMSG_CUDA(cudaMemcpy(h->up_off.p, hi.up_off.data(), n * 8, cudaMemcpyHostToDevice), "upload offsets");
+  NMSG_CUDA(cudaMemcpy(h->up_links.p, links.data(), links.size() * 4, cudaMemcpyHostToDevice), "upload links");
+  NMSG_CUDA(cudaMemcpy(h->ext_id.p, ext.data(), n * 4, cudaMemcpyHostToDevice), "upload ids");
+  d.vecs = h->vecs.as<float>();
+  d.l0 = h->l0.as<int32_t>();
+  d.up_off = h->up_off.as<int64_t>();
+  d.up_links = h->up_links.as<int32_t>();
+  d.ext_id = h->ext_id.as<int32_t>();
+  h->resident_bytes = (int64_t)(vec.size() * 4 + l0.size() * 4 + n * 12 + links.size() * 4);
+  return NMSG_OK;
+}
+
+int space_matches(int space, int dist_type) {
+  switch (space) {
+    case NMSG_SPACE_L2: return dist_type == kL2Sqr16Ext || dist_type == kL2SqrExt;
+    case NMSG_SPACE_COSINE: return dist_type == kNormCosine;
+    case NMSG_SPACE_NEGDOT: return dist_type == kNegDot;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nmsg_last_error(void) { return g_err.c_str(); }
+
+int nmsg_index_load(const char* path, int space, int device, nmsg_index** out) {
+  if (!out || !path) return fail(NMSG_ERR_BAD_ARG, "null argument");
+  *out = nullptr;
+  if (space < 0 || space > 2) return fail(NMSG_ERR_BAD_ARG, "unknown space code");
+  auto* h = new nmsg_index();
+  h->device = device;
+  h->space = space;
+  std::string err;
+  int rc = read_index_file(path, h->host, err);
+  if (rc == NMSG_OK) rc = validate_index(h->host, err);
+  if (rc == NMSG_OK && !h->host.empty_regular && h->host.n > 0 && !space_matches(space, h->host.dist_type)) {
+    rc = NMSG_ERR_BAD_ARG;
+    err = "the index file was built for a different space (distance code " + std::to_string(h->host.dist_type) + ")";
+  }
+  if (rc != NMSG_OK) {
+    delete h;
+    return fail(rc, err);
+  }
+  // the file is read and validated before any device is touched
+  int ndev = 0;
+  cudaError_t ce = cudaGetDeviceCount(&ndev);
+  if (ce != cudaSuccess || ndev == 0) {
+    delete h;
+    return fail(NMSG_ERR_DEVICE, "no CUDA device is available");
+  }
+  if (device < 0 || device >= ndev) {
+    delete h;
+    return fail(NMSG_ERR_BAD_ARG, "device ordinal out of range");
+  }
+  {
+    DeviceGuard g(device);
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+    rc = upload_index(h);
+  }
+  if (rc != NMSG_OK) {
+    nmsg_index_free(h);
+    return rc;
+  }
+  *out = h;
+  return NMSG_OK;
+}
+
+int nmsg_index_save(const nmsg_index* h, const char* path) {
+  if (!h || !path) return fail(NMSG_ERR_BAD_ARG, "null argument");
+  std::string err;
+  int rc = write_index_file(path, h->host, err);
+  return rc == NMSG_OK ? rc : fail(rc, err);
+}
+
+void nmsg_index_free(nmsg_index* h) {
+  if (!h) return;
+  {
+    DeviceGuard g(h->device);
+    for (DevBuf* b : {&h->vecs, &h->l0, &h->up_off, &h->up_links, &h->ext_id, &h->visited, &h->epochs, &h->locks,
+                      &h->old_heap, &h->counter, &h->status, &h->order, &h->kq, &h->efq, &h->q_stage,
+                      &h->ids_stage, &h->dists_stage, &h->counts_stage, &h->stats_stage})
+      b->release();
+  }
+  delete h;
+}
+
+int nmsg_index_info_get(const nmsg_index* h, nmsg_index_info* out) {
+  if (!h || !out) return fail(NMSG_ERR_BAD_ARG, "null argument");
+  out->n = h->host.n;
+  out->dim = h->host.dim;
+  out->dist_type = h->host.dist_type;
+  out->maxlevel = h->host.maxlevel;
+  out->enterpoint = (int32_t)h->host.enterpoint;
+  out->maxM = (int32_t)h->host.maxM;
+  out->maxM0 = (int32_t)h->host.maxM0;
+  out->ef = h->ef;
+  out->algo = h->algo;
+  out->device = h->device;
+  out->device_bytes = h->resident_bytes;
+  return NMSG_OK;
+}
+
+int nmsg_set_query_params(nmsg_index* h, int ef, int algo) {
+  if (!h) return fail(NMSG_ERR_BAD_ARG, "null index");
+  if (ef < 0) return fail(NMSG_ERR_BAD_ARG, "ef must be non-negative");
+  if (algo < 0 || algo > 2) return fail(NMSG_ERR_BAD_ARG, "algoType should be one of the following: old, v1merge");
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->ef = ef;
+  h->algo = algo;
+  return NMSG_OK;
+}
+
+int nmsg_last_device_status(const nmsg_index* h) { return h ? h->last_status : NMSG_ERR_BAD_ARG; }
+
+int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim, int32_t k,
+                   const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids, float* dists,
+                   int32_t* counts, int64_t* stats, uint32_t flags, void* stream) {
+  if (!h) return fail(NMSG_ERR_BAD_ARG, "Must call createIndex or loadIndex before this method");
+  if (nq < 0) return fail(NMSG_ERR_BAD_ARG, "negative query count");
+  if (nq > 0 && (!queries || !ids || !dists || !counts)) return fail(NMSG_ERR_BAD_ARG, "null buffer");
+  const bool dev_ptrs = flags & NMSG_DEVICE_PTRS;
+  if (dev_ptrs && (k_per_q || ef_per_q))
+    return fail(NMSG_ERR_BAD_ARG, "per-query k/ef arrays are host arrays; pass host buffers for mixed batches");
+  std::lock_guard<std::mutex> lk(h->mu);
+  const int ef = h->ef, algo = h->algo;
+  // per-query parameters and capacity of the shared-memory region
+  int region = 1;
+  bool any_old = false;
+  for (int64_t i = 0; i < nq; ++i) {
+    const int kq = k_per_q ? k_per_q[i] : k;
+    const int eq = ef_per_q ? ef_per_q[i] : ef;
+    if (kq < 1) return fail(NMSG_ERR_BAD_ARG, "k must be at least 1");
+    if (kq > kmax) return fail(NMSG_ERR_BAD_ARG, "k exceeds the output row stride kmax");
+    if (eq < 0) return fail(NMSG_ERR_BAD_ARG, "ef must be non-negative");
+    const bool old = algo == NMSG_ALGO_OLD || (algo == NMSG_ALGO_HYBRID && eq >= 1000);
+    any_old |= old;
+    region = std::max(region, old ? eq + 1 + kq : std::max(eq, kq));
+    if (!k_per_q && !ef_per_q) break;  // uniform batch: one check covers every query
+  }
+  if (nq == 0) return NMSG_OK;
+  const DevIndex& d = h->dev;
+  if (d.n == 0) {  // empty index: every query returns nothing (hnsw.cc:721-723)
+    if (dev_ptrs) {
+      DeviceGuard g(h->device);
+      NMSG_CUDA(cudaMemsetAsync(counts, 0, nq * 4, (cudaStream_t)stream), "memset counts");
+      NMSG_CUDA(cudaMemsetAsync(ids, 0xff, nq * kmax * 4, (cudaStream_t)stream), "memset ids");
+    } else {
+      std::fill(counts, counts + nq, 0);
+      std::fill(ids, ids + nq * kmax, -1);
+      std::fill(dists, dists + nq * kmax, __builtin_inff());
+      if (stats) std::fill(stats, stats + nq * 4, 0);
+    }
+    return NMSG_OK;
+  }
+  if (dim != d.dim)
+    return fail(NMSG_ERR_BAD_ARG, "query dimension " + std::to_string(dim) + " does not match the index dimension " +
+                                      std::to_string(d.dim));
+  DeviceGuard g(h->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool plain = flags & NMSG_PLAIN_KERNEL;
+
+  SearchArgs a;
+  a.ix = d;
+  a.nq = nq;
+  a.k_default = k;
+  a.ef_default = ef;
+  a.algo = algo;
+  a.kmax = kmax;
+  a.nbpad = ((std::max(d.maxM, d.maxM0) + 1 + 31) / 32) * 32;
+  a.region_items = region;
+  a.warp_smem = warp_smem_bytes(d, region, a.nbpad);
+  int wpb = plain ? 1 : kWarpsPerBlock;
+  while (wpb > 1 && wpb * a.warp_smem > kMaxSmemPerBlock) wpb >>= 1;
+  if (wpb * a.warp_smem > kMaxSmemPerBlock)
+    return fail(NMSG_ERR_CAPACITY, "max(ef, k) = " + std::to_string(region) + " needs more shared memory per query than a block has");
+  int bps = 0;
+  int rc = plain ? occupancy_plain(a.warp_smem, &bps) : occupancy_batched(wpb, wpb * a.warp_smem, &bps);
+  if (rc != 0 || bps < 1) return fail(NMSG_ERR_DEVICE, "no resident block fits this configuration");
+  const int blocks = plain ? 0 : bps * h->num_sms;
+  const int slots = plain ? bps * h->num_sms : blocks * wpb;
+  // scratch
+  const int64_t vpitch = ((d.n + 15) / 16) * 16;
+  if (slots > h->slots || (int64_t)h->visited.bytes < (int64_t)slots * vpitch) {
+    h->visited.release();
+    h->epochs.release();
+    h->locks.release();
+    NMSG_CUDA(h->visited.ensure((size_t)slots * vpitch, true), "cudaMalloc(visited sets)");
+    NMSG_CUDA(h->epochs.ensure(slots, true), "cudaMalloc(epochs)");
+    NMSG_CUDA(h->locks.ensure((size_t)slots * 4, true), "cudaMalloc(slot locks)");
+    h->slots = slots;
+  }
+  if (any_old) {
+    const int64_t cap = std::min<int64_t>(d.n + 1, 1 << 17);
+    if (cap > h->old_cap || (int64_t)h->old_heap.bytes < (int64_t)h->slots * cap * 8) {
+      h->old_heap.release();
+      NMSG_CUDA(h->old_heap.ensure((size_t)h->slots * cap * 8, false), "cudaMalloc(SearchOld heaps)");
+      h->old_cap = cap;
+    }
+  }
+  NMSG_CUDA(h->counter.ensure(4, true), "cudaMalloc(counter)");
+  NMSG_CUDA(h->status.ensure(4, true), "cudaMalloc(status)");
+  a.visited = h->visited.as<uint8_t>();
+  a.visited_pitch = vpitch;
+  a.epochs = h->epochs.as<uint8_t>();
+  a.slot_locks = h->locks.as<int32_t>();
+  a.num_slots = slots;
+  a.old_heap = h->old_heap.as<uint2>();
+  a.old_heap_cap = h->old_cap;
+  a.work_counter = h->counter.as<int32_t>();
+  a.status = h->status.as<int32_t>();
+
+  // inputs / outputs
+  const size_t qbytes = (size_t)nq * dim * 4, obytes = (size_t)nq * kmax * 4;
+  if (dev_ptrs) {
+    a.queries = queries;
+    a.ids = ids;
+    a.dists = dists;
+    a.counts = counts;
+    a.stats = stats;
+  } else {
+    NMSG_CUDA(h->q_stage.ensure(qbytes, false), "cudaMalloc(query staging)");
+    NMSG_CUDA(h->ids_stage.ensure(obytes, false), "cudaMalloc(id staging)");
+    NMSG_CUDA(h->dists_stage.ensure(obytes, false), "cudaMalloc(distance staging)");
+    NMSG_CUDA(h->counts_stage.ensure((size_t)nq * 4, false), "cudaMalloc(count staging)");
+    if (stats) NMSG_CUDA(h->stats_stage.ensure((size_t)nq * 32, false), "cudaMalloc(stats staging)");
+    NMSG_CUDA(cudaMemcpyAsync(h->q_stage.p, queries, qbytes, cudaMemcpyHostToDevice, st), "copy queries");
+    a.queries = h->q_stage.as<float>();
+    a.ids = h->ids_stage.as<int32_t>();
+    a.dists = h->dists_stage.as<float>();
+    a.counts = h->counts_stage.as<int32_t>();
+    a.stats = stats ? h->stats_stage.as<int64_t>() : nullptr;
+    if (k_per_q) {
+      NMSG_CUDA(h->kq.ensure((size_t)nq * 4, false), "cudaMalloc(k per query)");
+      NMSG_CUDA(cudaMemcpyAsync(h->kq.p, k_per_q, nq * 4, cudaMemcpyHostToDevice, st), "copy k");
+      a.k_per_q = h->kq.as<int32_t>();
+    }
+    if (ef_per_q) {
+      NMSG_CUDA(h->efq.ensure((size_t)nq * 4, false), "cudaMalloc(ef per query)");
+      NMSG_CUDA(cudaMemcpyAsync(h->efq.p, ef_per_q, nq * 4, cudaMemcpyHostToDevice, st), "copy ef");
+      a.ef_per_q = h->efq.as<int32_t>();
+      // most expensive queries first, so the persistent warps finish together
+      std::vector<int32_t> order(nq);
+      std::iota(order.begin(), order.end(), 0);
+      std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return ef_per_q[x] > ef_per_q[y]; });
+      NMSG_CUDA(h->order.ensure((size_t)nq * 4, false), "cudaMalloc(order)");
+      NMSG_CUDA(cudaMemcpy(h->order.p, order.data(), nq * 4, cudaMemcpyHostToDevice), "copy order");
+      a.order = h->order.as<int32_t>();
+    }
+  }
+  NMSG_CUDA(cudaMemsetAsync(a.work_counter, 0, 4, st), "reset counter");
+  NMSG_CUDA(cudaMemsetAsync(a.status, 0, 4, st), "reset status");
+  rc = plain ? launch_search_plain(a, stream) : launch_search_batched(a, blocks, wpb, stream);
+  if (rc != 0) return cuda_fail((cudaError_t)rc, "search kernel launch");
+  if (dev_ptrs) return NMSG_OK;
+  int32_t dstatus = 0;
+  NMSG_CUDA(cudaMemcpyAsync(ids, a.ids, obytes, cudaMemcpyDeviceToHost, st), "copy ids");
+  NMSG_CUDA(cudaMemcpyAsync(dists, a.dists, obytes, cudaMemcpyDeviceToHost, st), "copy distances");
+  NMSG_CUDA(cudaMemcpyAsync(counts, a.counts, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
+  if (stats) NMSG_CUDA(cudaMemcpyAsync(stats, a.stats, nq * 32, cudaMemcpyDeviceToHost, st), "copy stats");
+  NMSG_CUDA(cudaMemcpyAsync(&dstatus, a.status, 4, cudaMemcpyDeviceToHost, st), "copy status");
+  NMSG_CUDA(cudaStreamSynchronize(st), "search");
+  h->last_status = dstatus;
+  if (dstatus != 0) return fail(dstatus, "the search kernel reported a device-side error (status " + std::to_string(dstatus) + ")");
+  return NMSG_OK;
+}
+
+}  // extern "C"

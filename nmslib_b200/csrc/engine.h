@@ -1,0 +1,121 @@
+// Shared host/device declarations of the B200 HNSW query engine.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <vector_types.h>
+
+#ifdef __CUDACC__
+#define NMSG_HD __host__ __device__
+#else
+#define NMSG_HD
+#endif
+
+namespace nmsg {
+
+// Optimized-index distance codes (similarity_search/include/method/hnsw.h:50-58).
+enum DistCode { kL2Sqr16Ext = 1, kL2SqrExt = 2, kNormCosine = 3, kNegDot = 4 };
+
+// The index as read from an optimized HNSW file, in host memory.
+// File layout (similarity_search/src/method/hnsw.cc:774-806):
+//   u32 optimIndexFlag(=1) | u32 N | u64 memoryPerObject | u64 offsetLevel0 | u64 offsetData
+//   | i32 maxlevel | u32 enterpointId | u64 maxM | u64 maxM0 | i32 dist_func_type
+//   | u64 searchMethod | N * memoryPerObject level-0 block | per node: u32 sizemass + bytes.
+// Level-0 row i: [i32 ext id][i32 label][u64 datalength][dim x f32][i32 cnt][maxM0 x i32].
+struct HostIndex {
+  uint32_t n = 0;
+  uint64_t mem_per_obj = 0, off_level0 = 0, off_data = 0;
+  int32_t maxlevel = 0;
+  uint32_t enterpoint = 0;
+  uint64_t maxM = 0, maxM0 = 0;
+  int32_t dist_type = 0;
+  uint64_t search_method = 3;
+  int dim = 0;
+  bool empty_regular = false;        // the reference saves an empty index in the regular format
+  std::vector<char> level0;          // N * mem_per_obj bytes, verbatim
+  std::vector<uint32_t> link_bytes;  // per node sizemass
+  std::vector<int64_t> up_off;       // per node offset (ints) into up_links, -1 if level 0 only
+  std::vector<int32_t> up_links;     // concatenated upper-level lists, verbatim
+  std::vector<int32_t> level;        // per node top level
+
+  const float* vec(int64_t i) const {
+    return reinterpret_cast<const float*>(level0.data() + i * mem_per_obj + off_data + 16);
+  }
+  const int32_t* l0(int64_t i) const {
+    return reinterpret_cast<const int32_t*>(level0.data() + i * mem_per_obj + off_level0);
+  }
+  int32_t ext_id(int64_t i) const {
+    return *reinterpret_cast<const int32_t*>(level0.data() + i * mem_per_obj + off_data);
+  }
+};
+
+// Returns an nmsg_status code; `err` gets the message.
+int read_index_file(const char* path, HostIndex& ix, std::string& err);
+int validate_index(const HostIndex& ix, std::string& err);
+int write_index_file(const char* path, const HostIndex& ix, std::string& err);
+
+// Device-resident index. Vectors are stored with a row pitch of round_up(dim, 32) floats and,
+// inside each 32-float chunk of the first (dim & ~15) elements, permuted so that lane j of an
+// 8-lane group reads elements {j, j+8, j+16, j+24} of the chunk as one float4 — the exact
+// accumulation order of the reference's 8-wide AVX loop. Elements from (dim & ~15) on keep their
+// natural position. A final 16-float half chunk is permuted the same way into float2 pairs.
+struct DevIndex {
+  const float* vecs = nullptr;      // [n][pitch]
+  const int32_t* l0 = nullptr;      // [n][l0_pitch]: cnt, neighbour ids (internal)
+  const int64_t* up_off = nullptr;  // [n]
+  const int32_t* up_links = nullptr;
+  const int32_t* ext_id = nullptr;  // [n]
+  int64_t n = 0;
+  int dim = 0, pitch = 0, l0_pitch = 0;
+  int n16 = 0, n4 = 0;
+  int maxM = 0, maxM0 = 0, maxlevel = 0, enterpoint = 0, dist_type = 0;
+};
+
+// Position of element e of a vector in the permuted device row.
+NMSG_HD inline int permuted_pos(int e, int dim) {
+  const int n16 = dim & ~15;
+  if (e >= n16) return e;
+  const int c = e >> 5, r = e & 31, s = r >> 3, j = r & 7;
+  if (c * 32 + 32 <= n16) return c * 32 + j * 4 + s;
+  return c * 32 + j * 2 + s;  // final half chunk of 16
+}
+
+struct SearchArgs {
+  DevIndex ix;
+  const float* queries = nullptr;   // [nq][dim]
+  int64_t nq = 0;
+  int k_default = 10, ef_default = 20, algo = 0;
+  const int32_t* k_per_q = nullptr;
+  const int32_t* ef_per_q = nullptr;
+  const int32_t* order = nullptr;   // optional work order (query index per work item)
+  int kmax = 10;
+  int32_t* ids = nullptr;
+  float* dists = nullptr;
+  int32_t* counts = nullptr;
+  int64_t* stats = nullptr;         // optional [nq][4]
+  uint8_t* visited = nullptr;       // [num_slots][visited_pitch] epoch bytes
+  int64_t visited_pitch = 0;
+  uint8_t* epochs = nullptr;        // [num_slots]
+  int32_t* slot_locks = nullptr;    // [num_slots] (one-query-per-block kernel only)
+  int num_slots = 0;
+  uint2* old_heap = nullptr;        // [num_slots][old_heap_cap] SearchOld candidate heaps
+  int64_t old_heap_cap = 0;
+  int32_t* work_counter = nullptr;
+  int32_t* status = nullptr;
+  int region_items = 0;             // uint2 items per warp in the shared region
+  int nbpad = 32;                   // neighbour buffer length per warp
+  int warp_smem = 0;                // bytes of shared memory per warp
+};
+
+// Per-warp shared memory needed for the given caps.
+int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad);
+
+// Launchers (defined in hnsw_search.cu). Return a cudaError_t value.
+int launch_search_batched(const SearchArgs& a, int blocks, int warps_per_block, void* stream);
+int launch_search_plain(const SearchArgs& a, void* stream);
+int occupancy_batched(int warps_per_block, int smem_per_block, int* blocks_per_sm);
+int occupancy_plain(int smem_per_block, int* blocks_per_sm);
+
+}  // namespace nmsg

@@ -1,0 +1,370 @@
+// Host-side HNSW index builder: writes NMSLIB's optimized index file so that large workloads can
+// be indexed without the reference library. It follows the reference's construction algorithm
+// (similarity_search/src/method/hnsw.cc:183-470 CreateIndex, :534-609 add, :611-708
+// kSearchElementsWithAttemptsLevel; similarity_search/include/method/hnsw.h:129-169
+// getNeighborsByHeuristic2 and :258-314 addFriendlevel/link) with the same defaults
+// (maxM = M, maxM0 = 2M, mult = 1/ln M, delaunay_type 2, post 0) and the same packed layout
+// (hnsw.cc:353-465). Like the reference's multi-threaded build, the graph depends on thread
+// timing; node levels are a deterministic function of (seed, node).
+//
+// Construction distances are squared L2, 1 - dot on unit vectors (cosine) and -dot; the search
+// path never uses them, so they need not follow the reference's FMA lane order.
+#include <immintrin.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <queue>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "engine.h"
+#include "../../include/nmslib_b200.h"
+
+namespace nmsg {
+namespace {
+
+thread_local std::string g_build_err;
+
+__attribute__((target("avx2,fma"))) float dot_avx2(const float* a, const float* b, int d) {
+  __m256 s0 = _mm256_setzero_ps(), s1 = _mm256_setzero_ps();
+  int e = 0;
+  for (; e + 16 <= d; e += 16) {
+    s0 = _mm256_fmadd_ps(_mm256_loadu_ps(a + e), _mm256_loadu_ps(b + e), s0);
+    s1 = _mm256_fmadd_ps(_mm256_loadu_ps(a + e + 8), _mm256_loadu_ps(b + e + 8), s1);
+  }
+  for (; e + 8 <= d; e += 8) s0 = _mm256_fmadd_ps(_mm256_loadu_ps(a + e), _mm256_loadu_ps(b + e), s0);
+  s0 = _mm256_add_ps(s0, s1);
+  alignas(32) float t[8];
+  _mm256_store_ps(t, s0);
+  float s = ((t[0] + t[1]) + (t[2] + t[3])) + ((t[4] + t[5]) + (t[6] + t[7]));
+  for (; e < d; ++e) s += a[e] * b[e];
+  return s;
+}
+
+__attribute__((target("avx2,fma"))) float l2_avx2(const float* a, const float* b, int d) {
+  __m256 s0 = _mm256_setzero_ps(), s1 = _mm256_setzero_ps();
+  int e = 0;
+  for (; e + 16 <= d; e += 16) {
+    __m256 x = _mm256_sub_ps(_mm256_loadu_ps(a + e), _mm256_loadu_ps(b + e));
+    __m256 y = _mm256_sub_ps(_mm256_loadu_ps(a + e + 8), _mm256_loadu_ps(b + e + 8));
+    s0 = _mm256_fmadd_ps(x, x, s0);
+    s1 = _mm256_fmadd_ps(y, y, s1);
+  }
+  for (; e + 8 <= d; e += 8) {
+    __m256 x = _mm256_sub_ps(_mm256_loadu_ps(a + e), _mm256_loadu_ps(b + e));
+    s0 = _mm256_fmadd_ps(x, x, s0);
+  }
+  s0 = _mm256_add_ps(s0, s1);
+  alignas(32) float t[8];
+  _mm256_store_ps(t, s0);
+  float s = ((t[0] + t[1]) + (t[2] + t[3])) + ((t[4] + t[5]) + (t[6] + t[7]));
+  for (; e < d; ++e) {
+    const float x = a[e] - b[e];
+    s += x * x;
+  }
+  return s;
+}
+
+struct SpinLock {
+  std::atomic<uint8_t> f{0};
+  void lock() {
+    while (f.exchange(1, std::memory_order_acquire)) {
+      while (f.load(std::memory_order_relaxed)) _mm_pause();
+    }
+  }
+  void unlock() { f.store(0, std::memory_order_release); }
+};
+
+struct Builder {
+  const float* data = nullptr;  // n x dim (normalised copy for cosine)
+  std::vector<float> normed;
+  int64_t n = 0;
+  int dim = 0, space = 0, M = 16, maxM = 16, maxM0 = 32, efc = 200;
+  double mult = 0;
+  uint64_t seed = 0;
+  std::vector<int32_t> level;
+  std::vector<int32_t> l0;                 // n x (maxM0 + 1): cnt, ids
+  std::vector<std::vector<int32_t>> up;    // per node: level x (maxM + 1)
+  std::unique_ptr<SpinLock[]> locks;
+  std::atomic<int32_t> enterpoint{0};
+  std::atomic<int32_t> maxlevel{0};
+  std::mutex maxlevel_guard;
+
+  float dist(int64_t a, int64_t b) const { return dist_vec(data + a * dim, b); }
+  float dist_vec(const float* q, int64_t b) const {
+    const float* v = data + b * dim;
+    if (space == NMSG_SPACE_L2) return l2_avx2(q, v, dim);
+    const float d = dot_avx2(q, v, dim);
+    return space == NMSG_SPACE_COSINE ? 1.0f - d : -d;
+  }
+  int32_t* list(int64_t node, int lev) {
+    return lev == 0 ? l0.data() + node * (maxM0 + 1) : up[node].data() + (maxM + 1) * (lev - 1);
+  }
+  int cap(int lev) const { return lev == 0 ? maxM0 : maxM; }
+
+  int random_level(int64_t node) const {
+    // splitmix64 of (seed, node) -> uniform in (0, 1]; level = floor(-ln(u) * mult)  (hnsw.h:478-483)
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(node + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = ((z >> 11) + 1) * (1.0 / 9007199254740992.0);
+    return (int)(-std::log(u) * mult);
+  }
+
+  // getNeighborsByHeuristic2 (hnsw.h:129-169): candidates sorted ascending by distance to the
+  // base point; keep a candidate unless a kept one is strictly closer to it than the base is.
+  void heuristic(std::vector<std::pair<float, int32_t>>& cand, int nn) const {
+    if ((int)cand.size() < nn) return;
+    std::sort(cand.begin(), cand.end());
+    std::vector<std::pair<float, int32_t>> keep;
+    for (const auto& c : cand) {
+      if ((int)keep.size() >= nn) break;
+      bool good = true;
+      for (const auto& k : keep) {
+        if (dist(k.second, c.second) < c.first) {
+          good = false;
+          break;
+        }
+      }
+      if (good) keep.push_back(c);
+    }
+    cand.swap(keep);
+  }
+
+  // addFriendlevel (hnsw.h:258-314): append; on overflow shrink with the heuristic to at most
+  // size-1 and store the survivors farthest first, as the reference's max-heap pop order does.
+  void add_friend(int64_t node, int lev, int32_t other) {
+    std::lock_guard<SpinLock> g(locks[node]);
+    int32_t* lst = list(node, lev);
+    for (int j = 1; j <= lst[0]; ++j)
+      if (lst[j] == other) return;
+    if (lst[0] < cap(lev)) {
+      lst[++lst[0]] = other;
+      return;
+    }
+    std::vector<std::pair<float, int32_t>> c;
+    c.reserve(lst[0] + 1);
+    for (int j = 1; j <= lst[0]; ++j) c.push_back({dist(node, lst[j]), lst[j]});
+    c.push_back({dist(node, other), other});
+    heuristic(c, (int)c.size() - 1);
+    std::sort(c.begin(), c.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    lst[0] = (int32_t)c.size();
+    for (size_t j = 0; j < c.size(); ++j) lst[1 + j] = c[j].second;
+  }
+
+  // kSearchElementsWithAttemptsLevel (hnsw.cc:611-708)
+  void search_layer(const float* q, int32_t ep, int lev, std::vector<uint32_t>& vis, uint32_t& epoch,
+                    std::vector<std::pair<float, int32_t>>& out) {
+    if (++epoch == 0) {
+      std::fill(vis.begin(), vis.end(), 0);
+      epoch = 1;
+    }
+    std::priority_queue<std::pair<float, int32_t>> result;                         // max-heap
+    std::priority_queue<std::pair<float, int32_t>, std::vector<std::pair<float, int32_t>>,
+                        std::greater<std::pair<float, int32_t>>> cand;             // min-heap
+    const float d0 = dist_vec(q, ep);
+    result.push({d0, ep});
+    cand.push({d0, ep});
+    vis[ep] = epoch;
+    std::vector<int32_t> nb;
+    while (!cand.empty()) {
+      const auto cur = cand.top();
+      if (cur.first > result.top().first) break;
+      cand.pop();
+      {
+        std::lock_guard<SpinLock> g(locks[cur.second]);
+        const int32_t* lst = list(cur.second, lev);
+        nb.assign(lst + 1, lst + 1 + lst[0]);
+      }
+      for (int32_t id : nb) {
+        if (vis[id] == epoch) continue;
+        vis[id] = epoch;
+        const float d = dist_vec(q, id);
+        if ((int)result.size() < efc || result.top().first > d) {
+          result.push({d, id});
+          cand.push({d, id});
+          if ((int)result.size() > efc) result.pop();
+        }
+      }
+    }
+    out.clear();
+    while (!result.empty()) {
+      out.push_back(result.top());
+      result.pop();
+    }
+  }
+
+  // add (hnsw.cc:534-609)
+  void add(int64_t node, std::vector<uint32_t>& vis, uint32_t& epoch) {
+    const int cur_level = level[node];
+    std::unique_lock<std::mutex> top_lock;
+    if (cur_level > maxlevel.load()) top_lock = std::unique_lock<std::mutex>(maxlevel_guard);
+    const int maxl = maxlevel.load();
+    int32_t ep = enterpoint.load();
+    const float* q = data + node * dim;
+    if (cur_level < maxl) {
+      float curdist = dist_vec(q, ep);
+      for (int lev = maxl; lev > cur_level; --lev) {
+        bool changed = true;
+        while (changed) {
+          changed = false;
+          std::vector<int32_t> nb;
+          {
+            std::lock_guard<SpinLock> g(locks[ep]);
+            const int32_t* lst = list(ep, lev);
+            nb.assign(lst + 1, lst + 1 + lst[0]);
+          }
+          for (int32_t id : nb) {
+            const float d = dist_vec(q, id);
+            if (d < curdist) {
+              curdist = d;
+              ep = id;
+              changed = true;
+            }
+          }
+        }
+      }
+    }
+    std::vector<std::pair<float, int32_t>> res;
+    for (int lev = std::min(cur_level, maxl); lev >= 0; --lev) {
+      search_layer(q, ep, lev, vis, epoch, res);
+      heuristic(res, M);
+      // link farthest first; the closest becomes the entry for the next level
+      std::sort(res.begin(), res.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+      for (const auto& r : res) {
+        add_friend(r.second, lev, (int32_t)node);
+        add_friend(node, lev, r.second);
+      }
+      if (!res.empty()) ep = res.back().second;
+    }
+    if (cur_level > maxlevel.load()) {
+      enterpoint.store((int32_t)node);
+      maxlevel.store(cur_level);
+    }
+  }
+};
+
+}  // namespace
+}  // namespace nmsg
+
+using namespace nmsg;
+
+extern "C" NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t dim, const int32_t* ids,
+                                         int space, int M, int ef_construction, int nthreads, uint64_t seed,
+                                         const char* out_path) {
+  if (!data || n < 0 || dim <= 0 || !out_path || M < 2 || ef_construction < 1 || space < 0 || space > 2) {
+    g_build_err = "invalid build arguments";
+    return NMSG_ERR_BAD_ARG;
+  }
+  HostIndex out;
+  std::string err;
+  if (n == 0) {
+    out.empty_regular = true;
+    int rc = write_index_file(out_path, out, err);
+    if (rc) g_build_err = err;
+    return rc;
+  }
+  if (n > 0x7fffffffLL) {
+    g_build_err = "too many elements for int32 ids";
+    return NMSG_ERR_BAD_ARG;
+  }
+  Builder b;
+  b.n = n;
+  b.dim = dim;
+  b.space = space;
+  b.M = M;
+  b.maxM = M;
+  b.maxM0 = 2 * M;
+  b.efc = ef_construction;
+  b.mult = 1.0 / std::log(1.0 * M);
+  b.seed = seed;
+  b.data = data;
+  if (space == NMSG_SPACE_COSINE) {
+    // the reference stores unit vectors for cosine (hnsw.cc:441-446, NormalizeVect hnsw.h:486-497)
+    b.normed.assign(data, data + n * dim);
+    for (int64_t i = 0; i < n; ++i) {
+      float* v = b.normed.data() + i * dim;
+      float sum = 0;
+      for (int e = 0; e < dim; ++e) {
+        volatile float sq = v[e] * v[e];  // unfused, as the reference computes it
+        sum = sum + sq;
+      }
+      if (sum != 0.0f) {
+        const float s = 1.0f / std::sqrt(sum);
+        for (int e = 0; e < dim; ++e) v[e] *= s;
+      }
+    }
+    b.data = b.normed.data();
+  }
+  b.level.resize(n);
+  b.up.resize(n);
+  for (int64_t i = 0; i < n; ++i) {
+    b.level[i] = b.random_level(i);
+    if (b.level[i] > 0) b.up[i].assign((size_t)b.level[i] * (b.maxM + 1), 0);
+  }
+  b.l0.assign((size_t)n * (b.maxM0 + 1), 0);
+  b.locks.reset(new SpinLock[n]);
+  b.enterpoint = 0;
+  b.maxlevel = b.level[0];
+  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  std::atomic<int64_t> next(1);
+  auto worker = [&]() {
+    std::vector<uint32_t> vis(n, 0);
+    uint32_t epoch = 0;
+    for (;;) {
+      const int64_t i = next.fetch_add(1);
+      if (i >= n) break;
+      b.add(i, vis, epoch);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthreads; ++t) th.emplace_back(worker);
+  for (auto& t : th) t.join();
+
+  // pack the optimized layout (hnsw.cc:353-465)
+  out.n = (uint32_t)n;
+  out.dim = dim;
+  out.maxM = (uint64_t)b.maxM;
+  out.maxM0 = (uint64_t)b.maxM0;
+  out.off_data = 0;
+  out.off_level0 = 16 + 4ull * dim;
+  out.mem_per_obj = out.off_level0 + 4ull * (b.maxM0 + 1);
+  out.maxlevel = b.maxlevel.load();
+  out.enterpoint = (uint32_t)b.enterpoint.load();
+  out.dist_type = space == NMSG_SPACE_L2 ? (dim % 16 == 0 ? kL2Sqr16Ext : kL2SqrExt)
+                                         : (space == NMSG_SPACE_COSINE ? kNormCosine : kNegDot);
+  out.search_method = 3;
+  out.level0.assign(n * out.mem_per_obj, 1);  // padding bytes are 0x01, as memset(..., 1) leaves them
+  out.link_bytes.assign(n, 0);
+  out.up_off.assign(n, -1);
+  out.level = b.level;
+  for (int64_t i = 0; i < n; ++i) {
+    char* row = out.level0.data() + i * out.mem_per_obj;
+    const int32_t ext = ids ? ids[i] : (int32_t)i;
+    const int32_t label = -1;
+    const uint64_t dl = 4ull * dim;
+    std::memcpy(row, &ext, 4);
+    std::memcpy(row + 4, &label, 4);
+    std::memcpy(row + 8, &dl, 8);
+    std::memcpy(row + 16, b.data + i * dim, 4ull * dim);
+    const int32_t* lst = b.l0.data() + i * (b.maxM0 + 1);
+    std::memcpy(row + out.off_level0, lst, 4ull * (1 + lst[0]));
+    if (b.level[i] > 0) {
+      out.up_off[i] = (int64_t)out.up_links.size();
+      out.link_bytes[i] = (uint32_t)(b.up[i].size() * 4);
+      out.up_links.insert(out.up_links.end(), b.up[i].begin(), b.up[i].end());
+    }
+  }
+  int rc = write_index_file(out_path, out, err);
+  if (rc) g_build_err = err;
+  return rc;
+}
+
+extern "C" NMSG_API const char* nmsg_build_last_error(void) { return g_build_err.c_str(); }

@@ -1,0 +1,903 @@
+// HNSW query kernels for sm_100a: upper-level greedy descent, level-0 beam search with the
+// reference's SearchV1Merge and SearchOld semantics, and the warp-cooperative distances they use.
+//
+// One warp owns one query at a time. Everything the reference keeps per query — the query
+// vector, the sorted candidate array (SortArrBI), the neighbour buffer, SearchOld's heaps —
+// lives in the warp's slice of shared memory; the visited set is a per-warp epoch byte array in
+// HBM (the reference's VisitedList, similarity_search/include/method/hnsw.h:568-590), and
+// SearchOld's unbounded candidate heap spills to a per-warp HBM area.
+//
+// Arithmetic matches the reference bit for bit:
+//  * distances follow the AVX kernels of similarity_search/include/method/hnsw_distfunc_opt_impl_inline.h:42-173
+//    (8 accumulators fed by FMAs in element order, left-to-right lane sums, a 4-wide fused
+//    remainder and a scalar fused tail), computed by 8 lanes, lane j owning accumulator j;
+//  * the cosine query is normalised as in hnsw.h:486-497 (unfused sum of squares, 1/sqrtf);
+//  * every rounding step is an explicit __f*_rn intrinsic, so nvcc's contraction cannot
+//    change the result.
+// Tie order matches too: neighbour batches are ordered exactly as libstdc++ std::sort orders
+// them (stable rank sort where that is provably identical, a restatement of libstdc++'s
+// introsort otherwise), and insertion follows push_or_replace_non_empty_exp
+// (similarity_search/include/sort_arr_bi.h:159-199) including its exponential probe.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "engine.h"
+#include "../../include/nmslib_b200.h"
+
+namespace nmsg {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kUsedBit = 0x80000000u;
+constexpr uint32_t kIdMask = 0x7fffffffu;
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
+__device__ __forceinline__ float key_of(uint2 it) { return __uint_as_float(it.x); }
+__device__ __forceinline__ uint2 make_item(float key, int id, bool used) {
+  return make_uint2(__float_as_uint(key), (uint32_t)id | (used ? kUsedBit : 0u));
+}
+
+__device__ __forceinline__ void set_status(int32_t* status, int code) { atomicCAS(status, 0, code); }
+
+// ------------------------------------------------------------------ distances
+// Row and query are in the permuted layout (engine.h). `acc` is lane j's accumulator of the
+// 8-wide loop; the combine step reproduces the reference's reduction for each distance code.
+template <int R>
+struct RowAcc {
+  float acc[R];
+};
+
+__device__ __forceinline__ float fma_term(int code, float a, float b, float acc) {
+  if (code == kL2Sqr16Ext || code == kL2SqrExt) {
+    const float d = __fsub_rn(a, b);
+    return __fmaf_rn(d, d, acc);
+  }
+  return __fmaf_rn(a, b, acc);
+}
+
+// Reduce the 8 lane accumulators of one group into the reference's final value; every lane of
+// the group returns the same value. `row` and `q` are needed for the remainder elements.
+__device__ __forceinline__ float combine(const DevIndex& ix, float acc, const float* __restrict__ row,
+                                         const float* __restrict__ q) {
+  const int lane = lane_id();
+  const int gb = lane & ~7, j = lane & 7;
+  const int code = ix.dist_type;
+  if (code == kL2Sqr16Ext) {
+    // impl_inline.h:68-69: TmpRes[0] + ... + TmpRes[7], left to right
+    float s = __shfl_sync(kFull, acc, gb);
+#pragma unroll
+    for (int t = 1; t < 8; ++t) s = __fadd_rn(s, __shfl_sync(kFull, acc, gb + t));
+    return s;
+  }
+  // impl_inline.h:100,152: fold the 8 lanes to 4 (acc[j] + acc[j+4])
+  float t4 = __fadd_rn(acc, __shfl_down_sync(kFull, acc, 4, 8));
+  // 4-wide fused remainder over elements [n16, n4); lane j < 4 owns elements e == j (mod 4)
+  if (j < 4) {
+    for (int e = ix.n16 + j; e < ix.n4; e += 4) t4 = fma_term(code, q[e], __ldg(row + e), t4);
+  }
+  float s = __fadd_rn(__shfl_sync(kFull, t4, gb), __shfl_sync(kFull, t4, gb + 1));
+  s = __fadd_rn(s, __shfl_sync(kFull, t4, gb + 2));
+  s = __fadd_rn(s, __shfl_sync(kFull, t4, gb + 3));
+  // scalar fused tail over [n4, dim)
+  for (int e = ix.n4; e < ix.dim; ++e) s = fma_term(code, q[e], __ldg(row + e), s);
+  if (code == kNormCosine) {
+    // hnsw.cc:78-81: max(0, 1 - max(-1, min(1, dot))) with std::min/std::max operand order
+    const float mn = (s < 1.0f) ? s : 1.0f;
+    const float mx = (-1.0f < mn) ? mn : -1.0f;
+    const float v = __fsub_rn(1.0f, mx);
+    return (0.0f < v) ? v : 0.0f;
+  }
+  if (code == kNegDot) return -s;  // hnsw.cc:70-73
+  return s;
+}
+
+// Distances from the query (shared memory, permuted) to rows ids[0..n), written to out[0..n).
+// Four 8-lane groups per warp, R rows per group in flight.
+template <int R>
+__device__ void compute_dists(const DevIndex& ix, const float* __restrict__ q, const int* __restrict__ ids, int n,
+                              float* __restrict__ out) {
+  const int lane = lane_id();
+  const int g = lane >> 3, j = lane & 7;
+  const int nfull = ix.n16 >> 5;
+  const bool half = (ix.n16 & 31) != 0;
+  const int code = ix.dist_type;
+  for (int base = 0; base < n; base += 4 * R) {
+    const float* rows[R];
+    bool act[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int idx = base + g + 4 * r;
+      act[r] = idx < n;
+      rows[r] = ix.vecs + (int64_t)(act[r] ? ids[idx] : 0) * ix.pitch;
+    }
+    float acc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r] = 0.0f;
+#pragma unroll 4
+    for (int c = 0; c < nfull; ++c) {
+      const float4 qv = reinterpret_cast<const float4*>(q + c * 32)[j];
+      float4 x[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        x[r] = act[r] ? __ldg(reinterpret_cast<const float4*>(rows[r] + c * 32) + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        acc[r] = fma_term(code, qv.x, x[r].x, acc[r]);
+        acc[r] = fma_term(code, qv.y, x[r].y, acc[r]);
+        acc[r] = fma_term(code, qv.z, x[r].z, acc[r]);
+        acc[r] = fma_term(code, qv.w, x[r].w, acc[r]);
+      }
+    }
+    if (half) {
+      const float2 qv = reinterpret_cast<const float2*>(q + nfull * 32)[j];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const float2 x = act[r] ? __ldg(reinterpret_cast<const float2*>(rows[r] + nfull * 32) + j) : make_float2(0.f, 0.f);
+        acc[r] = fma_term(code, qv.x, x.x, acc[r]);
+        acc[r] = fma_term(code, qv.y, x.y, acc[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float d = combine(ix, acc[r], rows[r], q);
+      if (act[r] && j == 0) out[base + g + 4 * r] = d;
+    }
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------------ libstdc++ sort order
+// Restatement of the algorithm libstdc++ uses for std::sort on random-access ranges
+// (introsort with median-of-three pivot into the first slot, unguarded partition, a 16-element
+// threshold, heapsort fallback, final insertion sort). Comparison is on the key only, exactly as
+// SortArrBI::Item::operator< (sort_arr_bi.h:43-45). Single-lane code on shared memory; used for
+// neighbour batches that contain equal keys and more than 16 items.
+struct KV {
+  float* k;
+  int* v;
+  __device__ void swap(int a, int b) {
+    float tk = k[a];
+    k[a] = k[b];
+    k[b] = tk;
+    int tv = v[a];
+    v[a] = v[b];
+    v[b] = tv;
+  }
+};
+
+__device__ void lib_adjust_heap(KV a, int first, int hole, int len, float vk, int vv) {
+  const int top = hole;
+  int child = hole;
+  while (child < (len - 1) / 2) {
+    child = 2 * (child + 1);
+    if (a.k[first + child] < a.k[first + child - 1]) child--;
+    a.k[first + hole] = a.k[first + child];
+    a.v[first + hole] = a.v[first + child];
+    hole = child;
+  }
+  if ((len & 1) == 0 && child == (len - 2) / 2) {
+    child = 2 * (child + 1);
+    a.k[first + hole] = a.k[first + child - 1];
+    a.v[first + hole] = a.v[first + child - 1];
+    hole = child - 1;
+  }
+  int parent = (hole - 1) / 2;
+  while (hole > top && a.k[first + parent] < vk) {
+    a.k[first + hole] = a.k[first + parent];
+    a.v[first + hole] = a.v[first + parent];
+    hole = parent;
+    parent = (hole - 1) / 2;
+  }
+  a.k[first + hole] = vk;
+  a.v[first + hole] = vv;
+}
+
+__device__ void lib_heap_sort_range(KV a, int first, int last) {
+  const int len = last - first;
+  if (len >= 2) {  // make_heap
+    for (int parent = (len - 2) / 2;; --parent) {
+      lib_adjust_heap(a, first, parent, len, a.k[first + parent], a.v[first + parent]);
+      if (parent == 0) break;
+    }
+  }
+  for (int end = last; end - first > 1;) {  // sort_heap via pop_heap
+    --end;
+    const float vk = a.k[end];
+    const int vv = a.v[end];
+    a.k[end] = a.k[first];
+    a.v[end] = a.v[first];
+    lib_adjust_heap(a, first, 0, end - first, vk, vv);
+  }
+}
+
+__device__ void lib_move_median_to_first(KV a, int result, int x, int y, int z) {
+  if (a.k[x] < a.k[y]) {
+    if (a.k[y] < a.k[z])
+      a.swap(result, y);
+    else if (a.k[x] < a.k[z])
+      a.swap(result, z);
+    else
+      a.swap(result, x);
+  } else if (a.k[x] < a.k[z]) {
+    a.swap(result, x);
+  } else if (a.k[y] < a.k[z]) {
+    a.swap(result, z);
+  } else {
+    a.swap(result, y);
+  }
+}
+
+__device__ int lib_unguarded_partition(KV a, int first, int last, int pivot) {
+  while (true) {
+    while (a.k[first] < a.k[pivot]) ++first;
+    --last;
+    while (a.k[pivot] < a.k[last]) --last;
+    if (!(first < last)) return first;
+    a.swap(first, last);
+    ++first;
+  }
+}
+
+__device__ void lib_linear_insert(KV a, int last) {
+  const float vk = a.k[last];
+  const int vv = a.v[last];
+  int next = last - 1;
+  while (vk < a.k[next]) {
+    a.k[last] = a.k[next];
+    a.v[last] = a.v[next];
+    last = next;
+    --next;
+  }
+  a.k[last] = vk;
+  a.v[last] = vv;
+}
+
+__device__ void lib_insertion_sort(KV a, int first, int last) {
+  if (first == last) return;
+  for (int i = first + 1; i != last; ++i) {
+    if (a.k[i] < a.k[first]) {
+      const float vk = a.k[i];
+      const int vv = a.v[i];
+      for (int t = i; t > first; --t) {
+        a.k[t] = a.k[t - 1];
+        a.v[t] = a.v[t - 1];
+      }
+      a.k[first] = vk;
+      a.v[first] = vv;
+    } else {
+      lib_linear_insert(a, i);
+    }
+  }
+}
+
+__device__ void lib_std_sort(KV a, int n) {
+  if (n < 2) return;
+  int lg = 31 - __clz(n);
+  // introsort loop with an explicit stack instead of recursion on the right part
+  int stk_first[64], stk_last[64], stk_depth[64];
+  int sp = 0;
+  stk_first[sp] = 0;
+  stk_last[sp] = n;
+  stk_depth[sp] = 2 * lg;
+  ++sp;
+  while (sp > 0) {
+    --sp;
+    int first = stk_first[sp], last = stk_last[sp], depth = stk_depth[sp];
+    while (last - first > 16) {
+      if (depth == 0) {
+        lib_heap_sort_range(a, first, last);
+        break;
+      }
+      --depth;
+      const int mid = first + (last - first) / 2;
+      lib_move_median_to_first(a, first, first + 1, mid, last - 1);
+      const int cut = lib_unguarded_partition(a, first + 1, last, first);
+      // libstdc++ recurses on [cut, last) first, then loops on [first, cut); the two parts are
+      // disjoint, so processing order does not change the result.
+      // (segments of 16 or fewer are left to the final insertion sort, so only longer ones are
+      // stacked; stacked segments are disjoint and longer than 16, which bounds the stack)
+      if (last - cut > 16) {
+        stk_first[sp] = cut;
+        stk_last[sp] = last;
+        stk_depth[sp] = depth;
+        ++sp;
+      }
+      last = cut;
+    }
+  }
+  // final insertion sort
+  if (n > 16) {
+    lib_insertion_sort(a, 0, 16);
+    for (int i = 16; i < n; ++i) lib_linear_insert(a, i);
+  } else {
+    lib_insertion_sort(a, 0, n);
+  }
+}
+
+// Order sk/sv[0..n) as std::sort would. Warp-cooperative; tmpk/tmpv are scratch of length n.
+// Without equal keys every correct sort gives the same order, and for n <= 16 libstdc++ runs a
+// stable insertion sort, so a stable rank sort is exact in both cases; otherwise one lane runs
+// the restated introsort.
+__device__ void sort_like_std(float* sk, int* sv, int n, float* tmpk, int* tmpv) {
+  const int lane = lane_id();
+  bool tie = false;
+  for (int t = lane; t < n; t += 32) {
+    const float kt = sk[t];
+    int rank = 0;
+    for (int u = 0; u < n; ++u) {
+      const float ku = sk[u];
+      rank += (ku < kt) || (ku == kt && u < t);
+      tie |= (ku == kt && u != t);
+    }
+    tmpk[rank] = kt;
+    tmpv[rank] = sv[t];
+  }
+  const bool anytie = __any_sync(kFull, tie);
+  __syncwarp();
+  if (!anytie || n <= 16) {
+    for (int t = lane; t < n; t += 32) {
+      sk[t] = tmpk[t];
+      sv[t] = tmpv[t];
+    }
+  } else if (lane == 0) {
+    lib_std_sort(KV{sk, sv}, n);
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------------ sorted candidate array
+// push_or_replace_non_empty_exp (sort_arr_bi.h:159-199) over items[0..num) with capacity cap.
+// Returns the insertion index (num before the call when the item is appended, num when it is
+// dropped). Warp-cooperative; all lanes return the same values.
+__device__ int sorted_insert(uint2* items, int& num, int cap, float key, int id) {
+  const int lane = lane_id();
+  const float last_key = key_of(items[num - 1]);
+  if (last_key <= key) {
+    int ins = num;
+    if (num < cap) {
+      if (lane == 0) items[num] = make_item(key, id, false);
+      ++num;
+    }
+    __syncwarp();
+    return ins;
+  }
+  // The exponential probe from the tail visits num-1, num-2, num-4, ..., num-2^i (while > 0)
+  // and then stops at 0. It stops early at the first probe whose key is <= the new key.
+  const int c = (lane < 31) ? num - (1 << lane) : 0;
+  const bool valid = lane < 31 && c > 0;
+  const bool cond = valid && key_of(items[c]) <= key;
+  const unsigned cm = __ballot_sync(kFull, cond);
+  const unsigned vm = __ballot_sync(kFull, valid);
+  int p, prev;
+  if (cm) {
+    const int f = __ffs(cm) - 1;  // f >= 1: the probe at num-1 has a larger key
+    p = num - (1 << f);
+    prev = num - (1 << (f - 1));
+  } else {
+    p = 0;
+    prev = vm ? num - (1 << (31 - __clz(vm))) : 0;  // the last probe taken (none when num == 1)
+  }
+  int pos;
+  if (cm && key_of(items[p]) == key) {
+    pos = p;  // lower_bound over [p, prev) returns p itself
+  } else {
+    // lower_bound over [p, prev): count keys below `key` in that range (the array is sorted)
+    int cnt = 0;
+    for (int t = p + lane; t < prev; t += 32) cnt += key_of(items[t]) < key;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
+    pos = p + cnt;
+  }
+  // shift [pos, last) right by one; the tail item falls off when the array is full
+  const int last = (num < cap) ? num : num - 1;
+  for (int hi = last; hi > pos; hi -= 32) {
+    const int src = hi - 1 - lane;
+    const bool act = src >= pos;
+    uint2 v;
+    if (act) v = items[src];
+    __syncwarp();
+    if (act) items[src + 1] = v;
+    __syncwarp();
+  }
+  if (lane == 0) items[pos] = make_item(key, id, false);
+  if (num < cap) ++num;
+  __syncwarp();
+  return pos;
+}
+
+// ------------------------------------------------------------------ binary heaps (SearchOld)
+// std::priority_queue<EvaluatedMSWNodeInt> semantics (hnsw.h:410-431: ordered by distance only)
+// with libstdc++'s push_heap / pop_heap. Single-lane code.
+__device__ void heap_push(uint2* h, int& size, float key, int id) {
+  int hole = size++;
+  int parent = (hole - 1) / 2;
+  while (hole > 0 && key_of(h[parent]) < key) {
+    h[hole] = h[parent];
+    hole = parent;
+    parent = (hole - 1) / 2;
+  }
+  h[hole] = make_uint2(__float_as_uint(key), (uint32_t)id);
+}
+
+__device__ void heap_pop(uint2* h, int& size) {
+  if (size > 1) {
+    const int len = size - 1;
+    const uint2 value = h[len];
+    h[len] = h[0];
+    int hole = 0, child = 0;
+    while (child < (len - 1) / 2) {
+      child = 2 * (child + 1);
+      if (key_of(h[child]) < key_of(h[child - 1])) child--;
+      h[hole] = h[child];
+      hole = child;
+    }
+    if ((len & 1) == 0 && child == (len - 2) / 2) {
+      child = 2 * (child + 1);
+      h[hole] = h[child - 1];
+      hole = child - 1;
+    }
+    int parent = (hole - 1) / 2;
+    while (hole > 0 && key_of(h[parent]) < key_of(value)) {
+      h[hole] = h[parent];
+      hole = parent;
+      parent = (hole - 1) / 2;
+    }
+    h[hole] = value;
+  }
+  --size;
+}
+
+// The k-bounded result queue (knnqueue.h:55-64 + knnquery.cc:67-75) kept as an array sorted by
+// (distance, node); node index stands in for the reference's Object* order. Single lane.
+__device__ void result_offer(uint2* res, int& size, int k, float d, int node) {
+  if (size >= k) {
+    if (!(key_of(res[size - 1]) > d)) return;
+    --size;  // pop the largest (distance, node) pair
+  }
+  int pos = size;
+  while (pos > 0) {
+    const float pk = key_of(res[pos - 1]);
+    const int pn = (int)res[pos - 1].y;
+    if (pk < d || (pk == d && pn < node)) break;
+    res[pos] = res[pos - 1];
+    --pos;
+  }
+  res[pos] = make_uint2(__float_as_uint(d), (uint32_t)node);
+  ++size;
+}
+
+// ------------------------------------------------------------------ per-query driver
+struct WarpCtx {
+  float* q;      // [pitch]
+  uint2* items;  // shared region (V1Merge array, or SearchOld closest heap + result set)
+  int* nb_id;    // [nbpad]
+  float* nb_d;   // [nbpad]
+  float* sk;     // [nbpad]
+  int* sv;       // [nbpad]
+  uint8_t* vis;  // HBM epoch bytes of this warp's slot
+  uint8_t epoch;
+  int64_t st_dist, st_expand, st_greedy, st_bytes;
+};
+
+__device__ void load_query(const SearchArgs& a, const WarpCtx& w, int64_t qi) {
+  const DevIndex& ix = a.ix;
+  const int lane = lane_id();
+  const float* src = a.queries + qi * ix.dim;
+  // zero padding first (the permuted chunks read whole float4 / float2 groups)
+  for (int e = lane; e < ix.pitch; e += 32) w.q[e] = 0.0f;
+  __syncwarp();
+  float s = 1.0f;
+  bool scale = false;
+  if (ix.dist_type == kNormCosine) {
+    // hnsw.h:486-497, sequential and unfused
+    if (lane == 0) {
+      float sum = 0.0f;
+      for (int e = 0; e < ix.dim; ++e) {
+        const float v = src[e];
+        sum = __fadd_rn(sum, __fmul_rn(v, v));
+      }
+      if (sum != 0.0f) {
+        s = __fdiv_rn(1.0f, __fsqrt_rn(sum));
+        scale = true;
+      }
+    }
+    s = __shfl_sync(kFull, s, 0);
+    scale = __shfl_sync(kFull, scale, 0);
+  }
+  for (int e = lane; e < ix.dim; e += 32) {
+    float v = src[e];
+    if (scale) v = __fmul_rn(v, s);
+    w.q[permuted_pos(e, ix.dim)] = v;
+  }
+  __syncwarp();
+}
+
+// Mark unvisited neighbours of `list` (cnt ids) and gather them, in list order, into w.nb_id.
+// Returns how many were new. Duplicate ids inside one list count once (the first occurrence),
+// as the reference's sequential visited check does.
+__device__ int gather_new(const WarpCtx& w, const int32_t* list, int cnt) {
+  const int lane = lane_id();
+  int nnew = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    const int j = base + lane;
+    const int id = (j < cnt) ? __ldg(list + j) : -1;
+    const unsigned same = __match_any_sync(kFull, id);
+    const bool first = (__ffs(same) - 1) == lane;
+    bool isnew = false;
+    if (j < cnt && first) {
+      isnew = w.vis[id] != w.epoch;
+      if (isnew) w.vis[id] = w.epoch;
+    }
+    const unsigned m = __ballot_sync(kFull, isnew);
+    if (isnew) w.nb_id[nnew + __popc(m & lanemask_lt())] = id;
+    nnew += __popc(m);
+    __syncwarp();
+  }
+  return nnew;
+}
+
+template <int R>
+__device__ void greedy_descent(const SearchArgs& a, WarpCtx& w, int& cur_out, float& dist_out) {
+  const DevIndex& ix = a.ix;
+  const int lane = lane_id();
+  int cur = ix.enterpoint;
+  if (lane == 0) w.nb_id[0] = cur;
+  __syncwarp();
+  compute_dists<1>(ix, w.q, w.nb_id, 1, w.nb_d);
+  float curdist = w.nb_d[0];
+  w.st_dist += 1;
+  w.st_bytes += 4LL * ix.dim;
+  __syncwarp();
+  for (int lev = ix.maxlevel; lev > 0; --lev) {
+    bool changed = true;
+    while (changed) {
+      changed = false;
+      const int32_t* lst = ix.up_links + ix.up_off[cur] + (int64_t)(ix.maxM + 1) * (lev - 1);
+      const int cnt = __ldg(lst);
+      for (int t = lane; t < cnt; t += 32) w.nb_id[t] = __ldg(lst + 1 + t);
+      __syncwarp();
+      compute_dists<R>(ix, w.q, w.nb_id, cnt, w.nb_d);
+      w.st_greedy += 1;
+      w.st_dist += cnt;
+      w.st_bytes += 4LL * (1 + cnt) + 4LL * ix.dim * cnt;
+      // sequential scan with strict improvement == earliest position of the minimum below curdist
+      float best = curdist;
+      int bpos = 0x7fffffff;
+      for (int t = lane; t < cnt; t += 32) {
+        const float d = w.nb_d[t];
+        if (d < best || (d == best && d < curdist && t < bpos)) {
+          best = d;
+          bpos = t;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float ob = __shfl_xor_sync(kFull, best, o);
+        const int op = __shfl_xor_sync(kFull, bpos, o);
+        if (ob < best || (ob == best && op < bpos)) {
+          best = ob;
+          bpos = op;
+        }
+      }
+      if (bpos != 0x7fffffff && best < curdist) {
+        cur = w.nb_id[bpos];
+        curdist = best;
+        changed = true;
+      }
+      __syncwarp();
+    }
+  }
+  cur_out = cur;
+  dist_out = curdist;
+}
+
+__device__ void write_result_row(const SearchArgs& a, int64_t qi, const uint2* res, int cnt, bool node_sorted) {
+  // res[0..cnt) sorted by key; order equal keys by node index (the reference orders them by
+  // Object address, allocated in node order at load time, hnsw.cc:1071)
+  const int lane = lane_id();
+  const DevIndex& ix = a.ix;
+  for (int i = lane; i < a.kmax; i += 32) {
+    if (i < cnt) {
+      const float ki = key_of(res[i]);
+      const int ni = (int)(res[i].y & kIdMask);
+      int rank = i;
+      if (!node_sorted) {
+        int s = i;
+        while (s > 0 && key_of(res[s - 1]) == ki) --s;
+        int e = i + 1;
+        while (e < cnt && key_of(res[e]) == ki) ++e;
+        rank = s;
+        for (int t = s; t < e; ++t) rank += (int)(res[t].y & kIdMask) < ni;
+      }
+      a.ids[qi * a.kmax + rank] = __ldg(ix.ext_id + ni);
+      a.dists[qi * a.kmax + rank] = ki;
+    } else {
+      a.ids[qi * a.kmax + i] = -1;
+      a.dists[qi * a.kmax + i] = __int_as_float(0x7f800000);
+    }
+  }
+  if (lane == 0) a.counts[qi] = cnt;
+}
+
+template <int R>
+__device__ void search_v1merge(const SearchArgs& a, WarpCtx& w, int64_t qi, int k, int ef, int cur,
+                               float curdist) {
+  const DevIndex& ix = a.ix;
+  const int lane = lane_id();
+  const int cap = max(ef, k);
+  uint2* items = w.items;
+  int num = 1;
+  if (lane == 0) {
+    items[0] = make_item(curdist, cur, false);
+    w.vis[cur] = w.epoch;
+  }
+  __syncwarp();
+  int curr = 0;
+  while (curr < min(num, ef)) {
+    const uint2 e = items[curr];
+    const int node = (int)(e.y & kIdMask);
+    __syncwarp();
+    if (lane == 0) items[curr].y = e.y | kUsedBit;
+    __syncwarp();
+    ++curr;
+    const float top_key = key_of(items[num - 1]);
+    const int size_now = num;
+    const int32_t* lst = ix.l0 + (int64_t)node * ix.l0_pitch;
+    const int cnt = __ldg(lst);
+    w.st_expand += 1;
+    w.st_bytes += 4LL * (1 + cnt);
+    const int nnew = gather_new(w, lst + 1, cnt);
+    compute_dists<R>(ix, w.q, w.nb_id, nnew, w.nb_d);
+    w.st_dist += nnew;
+    w.st_bytes += 4LL * ix.dim * nnew;
+    // keep d < topKey || size < ef, preserving list order
+    int qty = 0;
+    for (int base = 0; base < nnew; base += 32) {
+      const int t = base + lane;
+      bool keep = false;
+      float d = 0.0f;
+      int id = 0;
+      if (t < nnew) {
+        d = w.nb_d[t];
+        id = w.nb_id[t];
+        keep = (d < top_key) || (size_now < ef);
+      }
+      const unsigned m = __ballot_sync(kFull, keep);
+      if (keep) {
+        const int p = qty + __popc(m & lanemask_lt());
+        w.sk[p] = d;
+        w.sv[p] = id;
+      }
+      qty += __popc(m);
+    }
+    __syncwarp();
+    if (qty) {
+      sort_like_std(w.sk, w.sv, qty, w.nb_d, w.nb_id);
+      for (int i = 0; i < qty; ++i) {
+        const int ins = sorted_insert(items, num, cap, w.sk[i], w.sv[i]);
+        if (ins < curr) curr = ins;
+      }
+    }
+    // advance to the first unused item
+    while (curr < num) {
+      const int t = curr + lane;
+      const bool unused = t < num && !(items[t].y & kUsedBit);
+      const unsigned m = __ballot_sync(kFull, unused);
+      if (m) {
+        curr += __ffs(m) - 1;
+        break;
+      }
+      curr += 32;
+      if (curr > num) curr = num;
+    }
+    __syncwarp();
+  }
+  const int cnt = min(k, num);
+  write_result_row(a, qi, items, cnt, false);
+}
+
+template <int R>
+__device__ bool search_old(const SearchArgs& a, WarpCtx& w, int64_t qi, int k, int ef, int cur, float curdist,
+                           uint2* cand) {
+  const DevIndex& ix = a.ix;
+  const int lane = lane_id();
+  uint2* closest = w.items;               // ef + 1 entries
+  uint2* res = w.items + (ef + 1);        // k entries
+  int csize = 0, rsize = 0, qsize = 0;    // closest, result, candidate sizes (lane 0's copy)
+  bool overflow = false;
+  if (lane == 0) {
+    heap_push(cand, qsize, -curdist, cur);
+    heap_push(closest, csize, curdist, cur);
+    result_offer(res, rsize, k, curdist, cur);
+    w.vis[cur] = w.epoch;
+  }
+  __syncwarp();
+  while (true) {
+    int node = -1;
+    if (lane == 0 && qsize > 0) {
+      const uint2 top = cand[0];
+      const float lb = key_of(closest[0]);
+      if (!(-key_of(top) > lb)) {
+        heap_pop(cand, qsize);
+        node = (int)top.y;
+      }
+    }
+    node = __shfl_sync(kFull, node, 0);
+    if (node < 0) break;
+    const int32_t* lst = ix.l0 + (int64_t)node * ix.l0_pitch;
+    const int cnt = __ldg(lst);
+    w.st_expand += 1;
+    w.st_bytes += 4LL * (1 + cnt);
+    const int nnew = gather_new(w, lst + 1, cnt);
+    compute_dists<R>(ix, w.q, w.nb_id, nnew, w.nb_d);
+    w.st_dist += nnew;
+    w.st_bytes += 4LL * ix.dim * nnew;
+    if (lane == 0) {
+      for (int t = 0; t < nnew; ++t) {
+        const float d = w.nb_d[t];
+        const int id = w.nb_id[t];
+        if (key_of(closest[0]) > d || csize < ef) {
+          if (qsize >= a.old_heap_cap) {
+            overflow = true;
+            break;
+          }
+          heap_push(cand, qsize, -d, id);
+          result_offer(res, rsize, k, d, id);
+          heap_push(closest, csize, d, id);
+          if (csize > ef) heap_pop(closest, csize);
+        }
+      }
+    }
+    overflow = __shfl_sync(kFull, overflow, 0);
+    __syncwarp();
+    if (overflow) break;
+  }
+  rsize = __shfl_sync(kFull, rsize, 0);
+  if (overflow) {
+    set_status(a.status, NMSG_ERR_CAPACITY);
+    rsize = 0;
+  }
+  write_result_row(a, qi, res, rsize, true);
+  return !overflow;
+}
+
+template <int R>
+__device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi) {
+  const DevIndex& ix = a.ix;
+  const int lane = lane_id();
+  WarpCtx w;
+  w.q = reinterpret_cast<float*>(wsmem);
+  w.items = reinterpret_cast<uint2*>(w.q + ix.pitch);
+  w.nb_id = reinterpret_cast<int*>(w.items + a.region_items);
+  w.nb_d = reinterpret_cast<float*>(w.nb_id + a.nbpad);
+  w.sk = w.nb_d + a.nbpad;
+  w.sv = reinterpret_cast<int*>(w.sk + a.nbpad);
+  w.vis = a.visited + (int64_t)slot * a.visited_pitch;
+  w.st_dist = w.st_expand = w.st_greedy = w.st_bytes = 0;
+
+  // next epoch of this slot's visited array; clear it when the byte wraps (hnsw.h:582-589)
+  int ep = 0;
+  if (lane == 0) ep = a.epochs[slot] + 1;
+  ep = __shfl_sync(kFull, ep, 0);
+  if (ep == 256) {
+    uint4* p = reinterpret_cast<uint4*>(w.vis);
+    const int64_t n16 = a.visited_pitch / 16;
+    for (int64_t t = lane; t < n16; t += 32) p[t] = make_uint4(0, 0, 0, 0);
+    ep = 1;
+    __syncwarp();
+  }
+  if (lane == 0) a.epochs[slot] = (uint8_t)ep;
+  w.epoch = (uint8_t)ep;
+
+  const int k = a.k_per_q ? a.k_per_q[qi] : a.k_default;
+  const int ef = a.ef_per_q ? a.ef_per_q[qi] : a.ef_default;
+  load_query(a, w, qi);
+  int cur;
+  float curdist;
+  greedy_descent<R>(a, w, cur, curdist);
+  const bool use_old = a.algo == NMSG_ALGO_OLD || (a.algo == NMSG_ALGO_HYBRID && ef >= 1000);
+  if (use_old) {
+    search_old<R>(a, w, qi, k, ef, cur, curdist, a.old_heap + (int64_t)slot * a.old_heap_cap);
+  } else {
+    search_v1merge<R>(a, w, qi, k, ef, cur, curdist);
+  }
+  if (a.stats && lane == 0) {
+    a.stats[qi * 4 + 0] = w.st_dist;
+    a.stats[qi * 4 + 1] = w.st_expand;
+    a.stats[qi * 4 + 2] = w.st_greedy;
+    a.stats[qi * 4 + 3] = w.st_bytes;
+  }
+  __syncwarp();
+}
+
+// Persistent kernel: each warp owns one slot and pulls queries from a work counter.
+template <int R>
+__global__ void __launch_bounds__(128) search_batched_kernel(SearchArgs a) {
+  extern __shared__ __align__(16) char smem[];
+  const int warp = threadIdx.x >> 5;
+  const int lane = lane_id();
+  char* wsmem = smem + warp * a.warp_smem;
+  const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (slot >= a.num_slots) return;
+  while (true) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(a.work_counter, 1);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= a.nq) break;
+    const int64_t qi = a.order ? a.order[item] : item;
+    run_query<R>(a, wsmem, slot, qi);
+  }
+}
+
+// One query per block of one warp; a free slot is taken from the slot locks for the duration.
+template <int R>
+__global__ void __launch_bounds__(32) search_plain_kernel(SearchArgs a) {
+  extern __shared__ __align__(16) char smem[];
+  const int lane = lane_id();
+  const int64_t qi = blockIdx.x;
+  int slot = -1;
+  if (lane == 0) {
+    // at most num_slots blocks are resident, so one pass over the locks finds a free slot
+    for (int t = 0; t < 2 * a.num_slots && slot < 0; ++t) {
+      const int s = (int)((blockIdx.x + t) % a.num_slots);
+      if (atomicCAS(a.slot_locks + s, 0, 1) == 0) slot = s;
+    }
+    __threadfence();
+  }
+  slot = __shfl_sync(kFull, slot, 0);
+  if (slot < 0) {
+    if (lane == 0) {
+      set_status(a.status, NMSG_ERR_TIMEOUT);
+      a.counts[qi] = 0;
+    }
+    return;
+  }
+  run_query<R>(a, smem, slot, qi);
+  __threadfence();
+  if (lane == 0) atomicExch(a.slot_locks + slot, 0);
+}
+
+constexpr int kRowsPerGroup = 2;
+
+}  // namespace
+
+int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad) {
+  int bytes = ix.pitch * 4 + region_items * 8 + nbpad * 16;
+  return (bytes + 15) & ~15;
+}
+
+int launch_search_batched(const SearchArgs& a, int blocks, int warps_per_block, void* stream) {
+  const int smem = a.warp_smem * warps_per_block;
+  auto kern = search_batched_kernel<kRowsPerGroup>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return (int)e;
+  kern<<<blocks, 32 * warps_per_block, smem, (cudaStream_t)stream>>>(a);
+  return (int)cudaGetLastError();
+}
+
+int launch_search_plain(const SearchArgs& a, void* stream) {
+  auto kern = search_plain_kernel<kRowsPerGroup>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, a.warp_smem);
+  if (e != cudaSuccess) return (int)e;
+  kern<<<(unsigned)a.nq, 32, a.warp_smem, (cudaStream_t)stream>>>(a);
+  return (int)cudaGetLastError();
+}
+
+int occupancy_batched(int warps_per_block, int smem_per_block, int* blocks_per_sm) {
+  auto kern = search_batched_kernel<kRowsPerGroup>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_per_block);
+  if (e != cudaSuccess) return (int)e;
+  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, 32 * warps_per_block,
+                                                            smem_per_block);
+}
+
+int occupancy_plain(int smem_per_block, int* blocks_per_sm) {
+  auto kern = search_plain_kernel<kRowsPerGroup>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_per_block);
+  if (e != cudaSuccess) return (int)e;
+  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, 32, smem_per_block);
+}
+
+}  // namespace nmsg

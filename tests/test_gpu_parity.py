@@ -1,0 +1,133 @@
+"""Parity of the CUDA engine (through the C ABI) with the oracle and with the reference's own
+recorded outputs, on every committed fixture. Distances must be bit-identical; ids identical to
+the oracle (both order equal distances by node index) and identical to the reference except
+inside runs of equal distance (the reference orders those by object address)."""
+import os
+
+import numpy as np
+import pytest
+
+import nmslib_b200 as nmslib
+from nmslib_b200.build import build
+from oracle.oracle import OracleIndex
+
+from conftest import ALGO_CODES, assert_same_results, golden_cases, golden_manifest, golden_path, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    build()
+
+
+_cache = {}
+
+
+def _gpu_index(name):
+    if name not in _cache:
+        space = golden_manifest()[name]["space"]
+        idx = nmslib.init(method="hnsw", space=space)
+        idx.loadIndex(golden_path(name))
+        _cache[name] = idx
+    return _cache[name]
+
+
+def _oracle(name):
+    key = ("oracle", name)
+    if key not in _cache:
+        _cache[key] = OracleIndex(golden_path(name))
+    return _cache[key]
+
+
+@pytest.mark.parametrize("plain", [False, True], ids=["batched", "plain"])
+@pytest.mark.parametrize("name,si,k,ef,algo", golden_cases())
+def test_gpu_matches_oracle_and_reference(name, si, k, ef, algo, plain):
+    g = load_golden(name)
+    q = g["queries"]
+    idx = _gpu_index(name)
+    idx.setQueryTimeParams({"efSearch": ef, "algoType": algo})
+    ids, d, cnt, st = idx.knnQueryBatchArrays(q, k, plain=plain, stats=True)
+    oi, od, oc, ost = _oracle(name).search(q, k=k, ef=ef, algo=ALGO_CODES[algo])
+    np.testing.assert_array_equal(cnt, oc)
+    np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
+    np.testing.assert_array_equal(ids, oi)
+    np.testing.assert_array_equal(st, ost)  # same distance evaluations, expansions, bytes
+    assert_same_results(ids, d, cnt, g[f"ids_{si}"], g[f"dists_{si}"], g[f"counts_{si}"])
+
+
+def test_mixed_batch_matches_oracle():
+    """One launch with per-query k and ef (both V1Merge and SearchOld queries)."""
+    rng = np.random.default_rng(7)
+    for name in ("c1_l2_d128", "sift_l2_ties", "negdot_d960"):
+        q = load_golden(name)["queries"]
+        k = rng.choice([1, 10, 100], size=len(q)).astype(np.int32)
+        ef = rng.integers(16, 1100, size=len(q)).astype(np.int32)
+        idx = _gpu_index(name)
+        idx.setQueryTimeParams({"efSearch": 20})
+        ids, d, cnt, st = idx.knnQueryBatchArrays(q, k, ef=ef, stats=True)
+        oi, od, oc, ost = _oracle(name).search(q, k_per_q=k, ef_per_q=ef)
+        np.testing.assert_array_equal(cnt, oc)
+        np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
+        np.testing.assert_array_equal(ids, oi)
+        np.testing.assert_array_equal(st, ost)
+
+
+def test_repeat_is_deterministic():
+    idx = _gpu_index("sift_l2_ties")
+    idx.setQueryTimeParams({"efSearch": 64})
+    q = load_golden("sift_l2_ties")["queries"]
+    a = idx.knnQueryBatchArrays(q, 10)
+    for _ in range(3):
+        b = idx.knnQueryBatchArrays(q, 10)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_python_surface_matches_reference_shapes(tmp_path):
+    g = load_golden("c1_l2_d128")
+    idx = nmslib.init(method="hnsw", space="l2")
+    idx.loadIndex(golden_path("c1_l2_d128"))
+    # after loadIndex ef is 20 (hnsw.cc:483): setting 1 of the fixture is ef=20
+    res = idx.knnQueryBatch(g["queries"][:50], k=10)
+    assert len(res) == 50
+    for r, (ri, rd) in enumerate(res):
+        assert ri.dtype == np.int32 and rd.dtype == np.float32
+        np.testing.assert_array_equal(rd, g["dists_1"][r])
+    # list input, Fortran-ordered input and knnQuery agree with the array path
+    a = idx.knnQueryBatch(np.asfortranarray(g["queries"][:5]), k=10)
+    b = idx.knnQueryBatch([list(v) for v in g["queries"][:5]], k=10)
+    c = [idx.knnQuery(v, k=10) for v in g["queries"][:5]]
+    for x, y, z in zip(a, b, c):
+        np.testing.assert_array_equal(x[0], y[0])
+        np.testing.assert_array_equal(x[0], z[0])
+    with pytest.raises(ValueError, match="dimension"):
+        idx.knnQueryBatch(np.zeros((2, 64), np.float32))
+    # save -> load round trip gives identical results
+    p = str(tmp_path / "re.hnsw")
+    idx.saveIndex(p)
+    with open(p, "rb") as f1, open(golden_path("c1_l2_d128"), "rb") as f2:
+        assert f1.read() == f2.read()
+    idx2 = nmslib.init(method="hnsw", space="l2")
+    idx2.loadIndex(p)
+    res2 = idx2.knnQueryBatch(g["queries"][:50], k=10)
+    for x, y in zip(res, res2):
+        np.testing.assert_array_equal(x[0], y[0])
+
+
+def test_empty_index(tmp_path):
+    import struct
+    p = tmp_path / "empty.hnsw"
+    p.write_bytes(struct.pack("<IIiiQQQ", 0, 0, 0, 0, 0, 0, 0))
+    idx = nmslib.init(method="hnsw", space="l2")
+    idx.loadIndex(str(p))
+    res = idx.knnQueryBatch(np.zeros((3, 5), np.float32), k=4)
+    assert [len(r[0]) for r in res] == [0, 0, 0]
+
+
+def test_zero_query_cosine():
+    """A zero query is left unnormalised and every cosine distance is 1 (bindings_test.py:72-91)."""
+    idx = _gpu_index("cos_d100")
+    idx.setQueryTimeParams({"efSearch": 50})
+    ids, d = idx.knnQuery(np.zeros(100, np.float32), k=5)
+    np.testing.assert_array_equal(d, np.ones(5, np.float32))
