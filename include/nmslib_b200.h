@@ -110,6 +110,33 @@ NMSG_API int nmsg_knn_batch(nmsg_index* index, const float* queries, int64_t nq,
                    const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids,
                    float* dists, int32_t* counts, int64_t* stats, uint32_t flags, void* stream);
 
+/* Build an HNSW index on the host and write it in the optimized format, like
+ * IndexWrapper::createIndex + saveIndex (python_bindings/nmslib.cc:89-96, :115-125)
+ * -> Hnsw::CreateIndex (similarity_search/src/method/hnsw.cc:183-470): M, efConstruction,
+ * maxM = M, maxM0 = 2M, mult = 1/ln M, neighbour heuristic 2. `ids` (optional) are the
+ * external ids (addDataPointBatch ids=...), else row numbers. nthreads <= 0: all cores.
+ * Node levels are a deterministic function of `seed`; the links depend on thread timing, as in
+ * the reference's multi-threaded build. */
+NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t dim, const int32_t* ids, int space, int M,
+                              int ef_construction, int nthreads, uint64_t seed, const char* out_path);
+
+NMSG_API const char* nmsg_build_last_error(void);
+
+/* Launch shape of the search kernels; 0 in a field = chosen automatically. */
+typedef struct nmsg_launch_config {
+  int32_t warps_per_block;   /* persistent kernel: 1, 2 or 4 queries (warps) per block */
+  int32_t rows_per_group;    /* register gather: vector rows each 8-lane group loads per round
+                                (1, 2 or 4) */
+  int32_t stage_rows;        /* staged gather: rows copied into shared memory per round with
+                                asynchronous copies (1..64); -1 = use the register gather */
+  int32_t visited_hash_log2; /* per-query shared-memory visited table of 2^x ids (8..14);
+                                -1 = visited set in HBM only */
+} nmsg_launch_config;
+
+/* Set (cfg != NULL) or reset to automatic (cfg == NULL) the launch shape used by later
+ * nmsg_knn_batch calls on this handle. Results do not depend on it; speed does. */
+NMSG_API int nmsg_set_launch_config(nmsg_index* index, const nmsg_launch_config* cfg);
+
 /* Device status of the last batch on this handle (NMSG_OK or a device-side error code). */
 NMSG_API int nmsg_last_device_status(const nmsg_index* index);
 

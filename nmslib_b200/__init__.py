@@ -89,18 +89,67 @@ class FloatIndex:
         self.dataType, self.distType = DataType(data_type), DistType(dtype)
         self._h = ctypes.c_void_p()
         self._info = None
+        self._data = []   # rows added with addDataPoint(Batch), consumed by createIndex
+        self._ids = []
 
     # ------------------------------------------------------------------ lifecycle
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _capi._lib is not None:
-            _capi._lib.nmsg_index_free(h)
-            self._h = ctypes.c_void_p()
+        lib = getattr(_capi, "_lib", None) if _capi is not None else None
+        if h and lib is not None:
+            lib.nmsg_index_free(h)
+            self._h = None
 
     def _require(self):
         if not self._h:
             raise ValueError("Must call createIndex or loadIndex before this method")
         return self._h
+
+    # ------------------------------------------------------------------ building
+    def addDataPointBatch(self, data, ids=None):
+        """IndexWrapper::addDataPointBatch (nmslib.cc:313-334): rows to index; ids default to the
+        row numbers. Returns the number of rows added."""
+        x = self._queries(data)
+        if ids is None:
+            start = sum(len(d) for d in self._data)
+            idv = np.arange(start, start + len(x), dtype=np.int64)
+        else:
+            idv = np.asarray(ids, dtype=np.int64).reshape(-1)
+            if len(idv) != len(x):
+                raise ValueError("ids must have one entry per row")
+        self._data.append(x)
+        self._ids.append(idv)
+        return len(x)
+
+    def addDataPoint(self, id, data):
+        self.addDataPointBatch(np.asarray(data, dtype=np.float32).reshape(1, -1), ids=[id])
+        return sum(len(d) for d in self._data) - 1
+
+    def createIndex(self, index_params=None, print_progress=False):
+        """IndexWrapper::createIndex (nmslib.cc:89-96) -> Hnsw::CreateIndex (hnsw.cc:183-470),
+        built on the host by the engine's builder (M, efConstruction, indexThreadQty; maxM = M,
+        maxM0 = 2M, heuristic 2) and loaded onto the device."""
+        p = _load_params(index_params)
+        known = {"M", "efConstruction", "indexThreadQty", "maxM", "maxM0", "delaunay_type", "post",
+                 "skip_optimized_index", "searchMethod", "seed"}
+        if set(p) - known:
+            raise RuntimeError("Unknown parameters found!")
+        m = _as_int("M", p.get("M", "16"))
+        efc = _as_int("efConstruction", p.get("efConstruction", "200"))
+        threads = _as_int("indexThreadQty", p.get("indexThreadQty", "0"))
+        if _as_int("maxM", p.get("maxM", str(m))) != m or _as_int("maxM0", p.get("maxM0", str(2 * m))) != 2 * m \
+                or p.get("delaunay_type", "2") != "2" or p.get("post", "0") != "0" \
+                or p.get("skip_optimized_index", "0") != "0":
+            raise ValueError("the B200 builder implements maxM=M, maxM0=2M, delaunay_type=2, post=0 and the "
+                             "optimized layout only")
+        data = np.concatenate(self._data) if self._data else np.zeros((0, 1), np.float32)
+        ids = np.concatenate(self._ids) if self._ids else np.zeros(0, np.int64)
+        import tempfile
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, "index.hnsw")
+            _capi.build_index(data, SPACES[self.space], m, efc, ids=ids.astype(np.int32), nthreads=threads,
+                              seed=_as_int("seed", p.get("seed", "0")), out_path=path)
+            self.loadIndex(path)
 
     def loadIndex(self, filename, load_data=False):
         """IndexWrapper::loadIndex (nmslib.cc:98-113): reads the optimized index file and resets
@@ -157,6 +206,11 @@ class FloatIndex:
         if "searchMethod" in p:
             _as_int("searchMethod", p["searchMethod"])
         _capi.check(_capi.load().nmsg_set_query_params(h, ef, _ALGOS[algo]))
+
+    def setLaunchConfig(self, warps_per_block=0, rows_per_group=0, visited_hash_log2=0, stage_rows=0):
+        """Launch shape of the search kernels (0 = automatic); results do not depend on it."""
+        cfg = _capi.LaunchConfig(warps_per_block, rows_per_group, stage_rows, visited_hash_log2)
+        _capi.check(_capi.load().nmsg_set_launch_config(self._require(), ctypes.byref(cfg)))
 
     # ------------------------------------------------------------------ search
     def _queries(self, input):

@@ -29,6 +29,11 @@ class IndexInfo(ctypes.Structure):
                 ("device", ctypes.c_int32), ("device_bytes", ctypes.c_int64)]
 
 
+class LaunchConfig(ctypes.Structure):
+    _fields_ = [("warps_per_block", ctypes.c_int32), ("rows_per_group", ctypes.c_int32),
+                ("stage_rows", ctypes.c_int32), ("visited_hash_log2", ctypes.c_int32)]
+
+
 _lib = None
 
 
@@ -60,8 +65,15 @@ def load(path: str = LIB_PATH):
     lib.nmsg_set_query_params.restype = ctypes.c_int
     lib.nmsg_knn_batch.argtypes = [P, P, I64, I32, I32, P, P, I32, P, P, P, P, U32, P]
     lib.nmsg_knn_batch.restype = ctypes.c_int
+    lib.nmsg_set_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
+    lib.nmsg_set_launch_config.restype = ctypes.c_int
     lib.nmsg_last_device_status.argtypes = [P]
     lib.nmsg_last_device_status.restype = ctypes.c_int
+    lib.nmsg_build_index.argtypes = [P, I64, I32, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_uint64, ctypes.c_char_p]
+    lib.nmsg_build_index.restype = ctypes.c_int
+    lib.nmsg_build_last_error.argtypes = []
+    lib.nmsg_build_last_error.restype = ctypes.c_char_p
     lib.nmsg_last_error.argtypes = []
     lib.nmsg_last_error.restype = ctypes.c_char_p
     _lib = lib
@@ -70,6 +82,22 @@ def load(path: str = LIB_PATH):
 
 def last_error() -> str:
     return load().nmsg_last_error().decode(errors="replace")
+
+
+def build_index(data, space: int, M: int = 16, ef_construction: int = 200, ids=None, nthreads: int = 0,
+                seed: int = 0, out_path: str = "index.hnsw"):
+    """Host HNSW build (nmsg_build_index) writing the reference's optimized file format."""
+    import numpy as np
+    lib = load()
+    x = np.ascontiguousarray(data, dtype=np.float32)
+    idv = None if ids is None else np.ascontiguousarray(ids, dtype=np.int32)
+    rc = lib.nmsg_build_index(x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1] if x.ndim == 2 else 0,
+                              None if idv is None else idv.ctypes.data_as(ctypes.c_void_p), space, M,
+                              ef_construction, nthreads, seed, os.fsencode(out_path))
+    if rc != OK:
+        msg = lib.nmsg_build_last_error().decode(errors="replace")
+        raise (ValueError if rc == ERR_BAD_ARG else RuntimeError)(msg)
+    return out_path
 
 
 def check(rc: int):

@@ -94,6 +94,7 @@ struct nmsg_index {
   int64_t old_cap = 0;      // entries per slot in old_heap
   int64_t resident_bytes = 0;
   int last_status = NMSG_OK;
+  nmsg_launch_config cfg{0, 0, 0, 0};
   std::mutex mu;
 };
 
@@ -253,6 +254,23 @@ int nmsg_set_query_params(nmsg_index* h, int ef, int algo) {
 
 int nmsg_last_device_status(const nmsg_index* h) { return h ? h->last_status : NMSG_ERR_BAD_ARG; }
 
+int nmsg_set_launch_config(nmsg_index* h, const nmsg_launch_config* cfg) {
+  if (!h) return fail(NMSG_ERR_BAD_ARG, "null index");
+  nmsg_launch_config c{0, 0, 0, 0};
+  if (cfg) {
+    c = *cfg;
+    const int w = c.warps_per_block, r = c.rows_per_group, hl = c.visited_hash_log2, sr = c.stage_rows;
+    if (!(w == 0 || w == 1 || w == 2 || w == 4)) return fail(NMSG_ERR_BAD_ARG, "warps_per_block must be 0, 1, 2 or 4");
+    if (!(r == 0 || r == 1 || r == 2 || r == 4)) return fail(NMSG_ERR_BAD_ARG, "rows_per_group must be 0, 1, 2 or 4");
+    if (!(sr == -1 || (sr >= 0 && sr <= 64))) return fail(NMSG_ERR_BAD_ARG, "stage_rows must be -1 or 0..64");
+    if (!(hl == 0 || hl == -1 || (hl >= 8 && hl <= 14)))
+      return fail(NMSG_ERR_BAD_ARG, "visited_hash_log2 must be 0, -1 or 8..14");
+  }
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->cfg = c;
+  return NMSG_OK;
+}
+
 int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim, int32_t k,
                    const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids, float* dists,
                    int32_t* counts, int64_t* stats, uint32_t flags, void* stream) {
@@ -275,7 +293,9 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
     if (eq < 0) return fail(NMSG_ERR_BAD_ARG, "ef must be non-negative");
     const bool old = algo == NMSG_ALGO_OLD || (algo == NMSG_ALGO_HYBRID && eq >= 1000);
     any_old |= old;
-    region = std::max(region, old ? eq + 1 + kq : std::max(eq, kq));
+    // V1Merge keeps its sorted array twice (merge target); SearchOld keeps its closest-set heap
+    // (ef + 1) and the k results
+    region = std::max(region, old ? eq + 1 + kq : 2 * std::max(eq, kq));
     if (!k_per_q && !ef_per_q) break;  // uniform batch: one check covers every query
   }
   if (nq == 0) return NMSG_OK;
@@ -308,14 +328,40 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
   a.algo = algo;
   a.kmax = kmax;
   a.nbpad = ((std::max(d.maxM, d.maxM0) + 1 + 31) / 32) * 32;
+  region = (region + 1) & ~1;  // keeps the following shared-memory pieces 16-byte aligned
   a.region_items = region;
-  a.warp_smem = warp_smem_bytes(d, region, a.nbpad);
-  int wpb = plain ? 1 : kWarpsPerBlock;
+  // launch shape: explicit configuration, else defaults by vector width and beam size
+  // Measured on B200 (1M x 128, 10K queries): staging 8 rows per round through shared memory is
+  // fastest for small beams (efSearch 64: 4.4M q/s vs 3.7M with register gathers), two rows per
+  // 8-lane group in registers for large ones (efSearch 256: 1.71M vs 1.67M).
+  int gather, stage_rows = 0;
+  const int beam = region / 2;
+  if (h->cfg.stage_rows > 0) {
+    gather = 0;
+    stage_rows = h->cfg.stage_rows;
+  } else if (h->cfg.stage_rows == 0 && h->cfg.rows_per_group == 0 && beam <= 160 && d.pitch <= 256) {
+    gather = 0;
+    stage_rows = 8;
+  } else {
+    gather = h->cfg.rows_per_group ? h->cfg.rows_per_group : (d.pitch <= 256 ? 2 : 1);
+  }
+  int hl = h->cfg.visited_hash_log2;
+  if (hl == 0) hl = -1;  // default: visited set in HBM (measured fastest at the default shapes)
+  a.hash_log2 = hl > 0 ? hl : 0;
+  a.stage_rows = stage_rows;
+  a.warp_smem = warp_smem_bytes(d, region, a.nbpad, a.hash_log2, stage_rows);
+  while (gather == 0 && stage_rows > 1 && a.warp_smem > kMaxSmemPerBlock) {  // wide rows: fewer per round
+    stage_rows = (stage_rows + 1) / 2;
+    a.stage_rows = stage_rows;
+    a.warp_smem = warp_smem_bytes(d, region, a.nbpad, a.hash_log2, stage_rows);
+  }
+  int wpb = plain ? 1 : (h->cfg.warps_per_block ? h->cfg.warps_per_block : kWarpsPerBlock);
   while (wpb > 1 && wpb * a.warp_smem > kMaxSmemPerBlock) wpb >>= 1;
   if (wpb * a.warp_smem > kMaxSmemPerBlock)
-    return fail(NMSG_ERR_CAPACITY, "max(ef, k) = " + std::to_string(region) + " needs more shared memory per query than a block has");
+    return fail(NMSG_ERR_CAPACITY, "max(ef, k) = " + std::to_string(region / 2) +
+                                       " needs more shared memory per query than a block has");
   int bps = 0;
-  int rc = plain ? occupancy_plain(a.warp_smem, &bps) : occupancy_batched(wpb, wpb * a.warp_smem, &bps);
+  int rc = search_occupancy(plain, gather, any_old, wpb, wpb * a.warp_smem, &bps);
   if (rc != 0 || bps < 1) return fail(NMSG_ERR_DEVICE, "no resident block fits this configuration");
   const int blocks = plain ? 0 : bps * h->num_sms;
   const int slots = plain ? bps * h->num_sms : blocks * wpb;
@@ -390,7 +436,7 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
   }
   NMSG_CUDA(cudaMemsetAsync(a.work_counter, 0, 4, st), "reset counter");
   NMSG_CUDA(cudaMemsetAsync(a.status, 0, 4, st), "reset status");
-  rc = plain ? launch_search_plain(a, stream) : launch_search_batched(a, blocks, wpb, stream);
+  rc = launch_search(a, plain, gather, any_old, blocks, wpb, stream);
   if (rc != 0) return cuda_fail((cudaError_t)rc, "search kernel launch");
   if (dev_ptrs) return NMSG_OK;
   int32_t dstatus = 0;

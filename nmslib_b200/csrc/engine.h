@@ -106,16 +106,21 @@ struct SearchArgs {
   int32_t* status = nullptr;
   int region_items = 0;             // uint2 items per warp in the shared region
   int nbpad = 32;                   // neighbour buffer length per warp
+  int hash_log2 = 0;                // shared-memory visited table of 2^hash_log2 ids (0: none)
+  int stage_rows = 0;               // rows per staged-gather round (gather mode 0)
   int warp_smem = 0;                // bytes of shared memory per warp
 };
 
 // Per-warp shared memory needed for the given caps.
-int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad);
+int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int hash_log2, int stage_rows);
 
-// Launchers (defined in hnsw_search.cu). Return a cudaError_t value.
-int launch_search_batched(const SearchArgs& a, int blocks, int warps_per_block, void* stream);
-int launch_search_plain(const SearchArgs& a, void* stream);
-int occupancy_batched(int warps_per_block, int smem_per_block, int* blocks_per_sm);
-int occupancy_plain(int smem_per_block, int* blocks_per_sm);
+// Launch / occupancy of the search kernels (defined in hnsw_search.cu). `gather` selects how
+// vector rows are fetched: 0 = asynchronous copies into shared memory (stage_rows per round),
+// 1/2/4 = registers, that many rows per 8-lane group. `with_old` includes the SearchOld path.
+// Return a cudaError_t value.
+int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, int blocks, int warps_per_block,
+                  void* stream);
+int search_occupancy(bool plain, int gather, bool with_old, int warps_per_block, int smem_per_block,
+                     int* blocks_per_sm);
 
 }  // namespace nmsg

@@ -75,13 +75,13 @@ __device__ __forceinline__ float combine(const DevIndex& ix, float acc, const fl
   float t4 = __fadd_rn(acc, __shfl_down_sync(kFull, acc, 4, 8));
   // 4-wide fused remainder over elements [n16, n4); lane j < 4 owns elements e == j (mod 4)
   if (j < 4) {
-    for (int e = ix.n16 + j; e < ix.n4; e += 4) t4 = fma_term(code, q[e], __ldg(row + e), t4);
+    for (int e = ix.n16 + j; e < ix.n4; e += 4) t4 = fma_term(code, q[e], row[e], t4);
   }
   float s = __fadd_rn(__shfl_sync(kFull, t4, gb), __shfl_sync(kFull, t4, gb + 1));
   s = __fadd_rn(s, __shfl_sync(kFull, t4, gb + 2));
   s = __fadd_rn(s, __shfl_sync(kFull, t4, gb + 3));
   // scalar fused tail over [n4, dim)
-  for (int e = ix.n4; e < ix.dim; ++e) s = fma_term(code, q[e], __ldg(row + e), s);
+  for (int e = ix.n4; e < ix.dim; ++e) s = fma_term(code, q[e], row[e], s);
   if (code == kNormCosine) {
     // hnsw.cc:78-81: max(0, 1 - max(-1, min(1, dot))) with std::min/std::max operand order
     const float mn = (s < 1.0f) ? s : 1.0f;
@@ -146,6 +146,62 @@ __device__ void compute_dists(const DevIndex& ix, const float* __restrict__ q, c
     }
   }
   __syncwarp();
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Distances to rows ids[0..n) through the warp's staging area: each round copies up to
+// `stage_rows` rows into shared memory with asynchronous 16-byte copies (every row of the round
+// in flight at once, no registers held), then the four 8-lane groups reduce them.
+__device__ void compute_dists_staged(const DevIndex& ix, const float* __restrict__ q, const int* __restrict__ ids,
+                                     int n, float* __restrict__ out, float* __restrict__ stage, int stage_rows) {
+  const int lane = lane_id();
+  const int g = lane >> 3, j = lane & 7;
+  const int nf4 = (ix.dim + 3) >> 2;  // 16-byte chunks covering elements [0, dim)
+  const int nfull = ix.n16 >> 5;
+  const bool half = (ix.n16 & 31) != 0;
+  const int code = ix.dist_type;
+  for (int base = 0; base < n; base += stage_rows) {
+    const int cnt = min(stage_rows, n - base);
+    for (int r = 0; r < cnt; ++r) {
+      const float* src = ix.vecs + (int64_t)ids[base + r] * ix.pitch;
+      float* dst = stage + r * ix.pitch;
+      for (int c = lane; c < nf4; c += 32) cp_async16(dst + 4 * c, src + 4 * c);
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    for (int r0 = 0; r0 < cnt; r0 += 4) {
+      const int r = r0 + g;
+      const bool act = r < cnt;
+      const float* row = stage + (act ? r : 0) * ix.pitch;
+      float acc = 0.0f;
+#pragma unroll 4
+      for (int c = 0; c < nfull; ++c) {
+        const float4 qv = reinterpret_cast<const float4*>(q + c * 32)[j];
+        const float4 x = reinterpret_cast<const float4*>(row + c * 32)[j];
+        acc = fma_term(code, qv.x, x.x, acc);
+        acc = fma_term(code, qv.y, x.y, acc);
+        acc = fma_term(code, qv.z, x.z, acc);
+        acc = fma_term(code, qv.w, x.w, acc);
+      }
+      if (half) {
+        const float2 qv = reinterpret_cast<const float2*>(q + nfull * 32)[j];
+        const float2 x = reinterpret_cast<const float2*>(row + nfull * 32)[j];
+        acc = fma_term(code, qv.x, x.x, acc);
+        acc = fma_term(code, qv.y, x.y, acc);
+      }
+      const float d = combine(ix, acc, row, q);
+      if (act && j == 0) out[base + r] = d;
+    }
+    __syncwarp();
+  }
 }
 
 // ------------------------------------------------------------------ libstdc++ sort order
@@ -407,6 +463,55 @@ __device__ int sorted_insert(uint2* items, int& num, int cap, float key, int id)
   return pos;
 }
 
+// Inserts a sorted batch sk/sv[0..m) into items[0..num) in one parallel pass, writing the result
+// to `spare`. Exact only when no key of the batch equals another batch key or a key already in
+// the array: then push_or_replace_non_empty_exp always lands on the lower bound, so sequential
+// insertion equals a stable merge truncated to `cap`, and the smallest returned insertion index is
+// the merged position of the first batch item. Returns false (nothing changed) when a tie exists.
+__device__ bool merge_batch(const uint2* items, uint2* spare, int num, int cap, const float* sk, const int* sv,
+                            int m, int* first_pos) {
+  const int lane = lane_id();
+  bool tie = false;
+  int p0 = cap;
+  for (int i = lane; i < m; i += 32) {
+    const float key = sk[i];
+    if (i + 1 < m && sk[i + 1] == key) tie = true;
+    int lo = 0, hi = num;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (key_of(items[mid]) < key)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if (lo < num && key_of(items[lo]) == key) tie = true;
+    const int p = lo + i;
+    if (i == 0) p0 = p;
+    if (p < cap) spare[p] = make_item(key, sv[i], false);
+  }
+  if (__any_sync(kFull, tie)) {
+    __syncwarp();
+    return false;
+  }
+  for (int t = lane; t < num; t += 32) {
+    const uint2 it = items[t];
+    const float key = key_of(it);
+    int lo = 0, hi = m;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (sk[mid] < key)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    const int p = t + lo;
+    if (p < cap) spare[p] = it;
+  }
+  *first_pos = __shfl_sync(kFull, p0, 0);
+  __syncwarp();
+  return true;
+}
+
 // ------------------------------------------------------------------ binary heaps (SearchOld)
 // std::priority_queue<EvaluatedMSWNodeInt> semantics (hnsw.h:410-431: ordered by distance only)
 // with libstdc++'s push_heap / pop_heap. Single-lane code.
@@ -476,10 +581,61 @@ struct WarpCtx {
   float* nb_d;   // [nbpad]
   float* sk;     // [nbpad]
   int* sv;       // [nbpad]
+  uint2* spare;  // V1Merge: second buffer of the sorted array (merge target)
+  float* stage;  // staged-gather rows (stage_rows x pitch), or null
+  int* htab;     // shared-memory visited table (open addressing, -1 = empty), or null
   uint8_t* vis;  // HBM epoch bytes of this warp's slot
   uint8_t epoch;
-  int64_t st_dist, st_expand, st_greedy, st_bytes;
+  int hshift;    // 32 - log2(table size)
+  int hmask;     // table size - 1
+  int hcount;    // ids in the table
+  int hlimit;    // entries allowed before the query spills to the HBM epoch bytes
+  bool spilled;
+  int st_dist, st_expand, st_greedy;
+  int64_t st_bytes;
 };
+
+// ------------------------------------------------------------------ visited set
+// Exact membership: the shared-memory table holds the first hlimit visited ids of a query;
+// after that the query "spills" and new ids go to the slot's HBM epoch bytes (the reference's
+// VisitedList scheme, hnsw.h:568-590). An id is visited iff it is in the table or, once
+// spilled, its epoch byte equals the query's epoch.
+__device__ __forceinline__ uint32_t hslot(const WarpCtx& w, int id) {
+  return ((uint32_t)id * 2654435761u) >> w.hshift;
+}
+
+// Inserts id; true if it was absent. The table always keeps a free slot (hcount <= hlimit <
+// size), so the probe ends.
+__device__ __forceinline__ bool hash_insert(const WarpCtx& w, int id) {
+  uint32_t h = hslot(w, id);
+  while (true) {
+    const int old = atomicCAS(w.htab + h, -1, id);
+    if (old == -1) return true;
+    if (old == id) return false;
+    h = (h + 1) & w.hmask;
+  }
+}
+
+__device__ __forceinline__ bool hash_contains(const WarpCtx& w, int id) {
+  uint32_t h = hslot(w, id);
+  while (true) {
+    const int v = w.htab[h];
+    if (v == id) return true;
+    if (v == -1) return false;
+    h = (h + 1) & w.hmask;
+  }
+}
+
+// Marks one id visited (lane 0 only); used for the level-0 entry point.
+__device__ void visit_one(WarpCtx& w, int id) {
+  if (w.htab) {
+    if (lane_id() == 0) hash_insert(w, id);
+    w.hcount += 1;
+  } else if (lane_id() == 0) {
+    w.vis[id] = w.epoch;
+  }
+  __syncwarp();
+}
 
 __device__ void load_query(const SearchArgs& a, const WarpCtx& w, int64_t qi) {
   const DevIndex& ix = a.ix;
@@ -514,19 +670,41 @@ __device__ void load_query(const SearchArgs& a, const WarpCtx& w, int64_t qi) {
   __syncwarp();
 }
 
-// Mark unvisited neighbours of `list` (cnt ids) and gather them, in list order, into w.nb_id.
-// Returns how many were new. Duplicate ids inside one list count once (the first occurrence),
-// as the reference's sequential visited check does.
-__device__ int gather_new(const WarpCtx& w, const int32_t* list, int cnt) {
+// Reads a level-0 list (count and ids in one round of independent loads), marks its unvisited
+// neighbours and gathers them, in list order, into w.nb_id. Returns how many were new; *cnt_out
+// gets the list length. Duplicate ids inside one list count once (the first occurrence), as the
+// reference's sequential visited check does (hnsw_distfunc_opt.cc:233-236).
+__device__ int expand_list(WarpCtx& w, const int32_t* lst, int maxcnt, int* cnt_out) {
   const int lane = lane_id();
+  int v[4];  // maxM0 <= 100 (validated at load) -> at most 4 chunks of 32
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int j = 32 * c + lane;
+    v[c] = (j < maxcnt) ? __ldg(lst + 1 + j) : -1;
+  }
+  const int cnt = __ldg(lst);
+  *cnt_out = cnt;
   int nnew = 0;
-  for (int base = 0; base < cnt; base += 32) {
-    const int j = base + lane;
-    const int id = (j < cnt) ? __ldg(list + j) : -1;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (32 * c >= cnt) break;
+    const int j = 32 * c + lane;
+    const int id = (j < cnt) ? v[c] : -1;
     const unsigned same = __match_any_sync(kFull, id);
-    const bool first = (__ffs(same) - 1) == lane;
+    const bool cand = j < cnt && (__ffs(same) - 1) == lane;
     bool isnew = false;
-    if (j < cnt && first) {
+    if (w.htab && !w.spilled) {
+      if (w.hcount + __popc(__ballot_sync(kFull, cand)) > w.hlimit) w.spilled = true;
+    }
+    if (!w.htab) {
+      if (cand) {
+        isnew = w.vis[id] != w.epoch;
+        if (isnew) w.vis[id] = w.epoch;
+      }
+    } else if (!w.spilled) {
+      if (cand) isnew = hash_insert(w, id);
+      w.hcount += __popc(__ballot_sync(kFull, isnew));
+    } else if (cand && !hash_contains(w, id)) {
       isnew = w.vis[id] != w.epoch;
       if (isnew) w.vis[id] = w.epoch;
     }
@@ -536,6 +714,18 @@ __device__ int gather_new(const WarpCtx& w, const int32_t* list, int cnt) {
     __syncwarp();
   }
   return nnew;
+}
+
+template <int G>
+__device__ __forceinline__ void dists(const SearchArgs& a, const WarpCtx& w, const int* ids, int n, float* out) {
+  if (G == 0)
+    compute_dists_staged(a.ix, w.q, ids, n, out, w.stage, a.stage_rows);
+  else
+    compute_dists<(G > 0 ? G : 1)>(a.ix, w.q, ids, n, out);
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
 template <int R>
@@ -558,7 +748,7 @@ __device__ void greedy_descent(const SearchArgs& a, WarpCtx& w, int& cur_out, fl
       const int cnt = __ldg(lst);
       for (int t = lane; t < cnt; t += 32) w.nb_id[t] = __ldg(lst + 1 + t);
       __syncwarp();
-      compute_dists<R>(ix, w.q, w.nb_id, cnt, w.nb_d);
+      dists<R>(a, w, w.nb_id, cnt, w.nb_d);
       w.st_greedy += 1;
       w.st_dist += cnt;
       w.st_bytes += 4LL * (1 + cnt) + 4LL * ix.dim * cnt;
@@ -628,12 +818,10 @@ __device__ void search_v1merge(const SearchArgs& a, WarpCtx& w, int64_t qi, int 
   const int lane = lane_id();
   const int cap = max(ef, k);
   uint2* items = w.items;
+  uint2* spare = w.spare;
   int num = 1;
-  if (lane == 0) {
-    items[0] = make_item(curdist, cur, false);
-    w.vis[cur] = w.epoch;
-  }
-  __syncwarp();
+  if (lane == 0) items[0] = make_item(curdist, cur, false);
+  visit_one(w, cur);
   int curr = 0;
   while (curr < min(num, ef)) {
     const uint2 e = items[curr];
@@ -644,12 +832,18 @@ __device__ void search_v1merge(const SearchArgs& a, WarpCtx& w, int64_t qi, int 
     ++curr;
     const float top_key = key_of(items[num - 1]);
     const int size_now = num;
+    // the next candidate in line is usually expanded next: start pulling its list into L2
+    if (lane < 2 && curr < num) {
+      const int nxt = (int)(items[curr].y & kIdMask);
+      const int32_t* p = ix.l0 + (int64_t)nxt * ix.l0_pitch + 32 * lane;
+      if (32 * lane < ix.l0_pitch) prefetch_l2(p);
+    }
     const int32_t* lst = ix.l0 + (int64_t)node * ix.l0_pitch;
-    const int cnt = __ldg(lst);
+    int cnt;
+    const int nnew = expand_list(w, lst, ix.maxM0, &cnt);
     w.st_expand += 1;
     w.st_bytes += 4LL * (1 + cnt);
-    const int nnew = gather_new(w, lst + 1, cnt);
-    compute_dists<R>(ix, w.q, w.nb_id, nnew, w.nb_d);
+    dists<R>(a, w, w.nb_id, nnew, w.nb_d);
     w.st_dist += nnew;
     w.st_bytes += 4LL * ix.dim * nnew;
     // keep d < topKey || size < ef, preserving list order
@@ -675,9 +869,18 @@ __device__ void search_v1merge(const SearchArgs& a, WarpCtx& w, int64_t qi, int 
     __syncwarp();
     if (qty) {
       sort_like_std(w.sk, w.sv, qty, w.nb_d, w.nb_id);
-      for (int i = 0; i < qty; ++i) {
-        const int ins = sorted_insert(items, num, cap, w.sk[i], w.sv[i]);
-        if (ins < curr) curr = ins;
+      int p0;
+      if (merge_batch(items, spare, num, cap, w.sk, w.sv, qty, &p0)) {
+        uint2* t = items;
+        items = spare;
+        spare = t;
+        num = min(num + qty, cap);
+        if (p0 < curr) curr = p0;
+      } else {
+        for (int i = 0; i < qty; ++i) {
+          const int ins = sorted_insert(items, num, cap, w.sk[i], w.sv[i]);
+          if (ins < curr) curr = ins;
+        }
       }
     }
     // advance to the first unused item
@@ -711,9 +914,8 @@ __device__ bool search_old(const SearchArgs& a, WarpCtx& w, int64_t qi, int k, i
     heap_push(cand, qsize, -curdist, cur);
     heap_push(closest, csize, curdist, cur);
     result_offer(res, rsize, k, curdist, cur);
-    w.vis[cur] = w.epoch;
   }
-  __syncwarp();
+  visit_one(w, cur);
   while (true) {
     int node = -1;
     if (lane == 0 && qsize > 0) {
@@ -727,11 +929,11 @@ __device__ bool search_old(const SearchArgs& a, WarpCtx& w, int64_t qi, int k, i
     node = __shfl_sync(kFull, node, 0);
     if (node < 0) break;
     const int32_t* lst = ix.l0 + (int64_t)node * ix.l0_pitch;
-    const int cnt = __ldg(lst);
+    int cnt;
+    const int nnew = expand_list(w, lst, ix.maxM0, &cnt);
     w.st_expand += 1;
     w.st_bytes += 4LL * (1 + cnt);
-    const int nnew = gather_new(w, lst + 1, cnt);
-    compute_dists<R>(ix, w.q, w.nb_id, nnew, w.nb_d);
+    dists<R>(a, w, w.nb_id, nnew, w.nb_d);
     w.st_dist += nnew;
     w.st_bytes += 4LL * ix.dim * nnew;
     if (lane == 0) {
@@ -763,7 +965,7 @@ __device__ bool search_old(const SearchArgs& a, WarpCtx& w, int64_t qi, int k, i
   return !overflow;
 }
 
-template <int R>
+template <int R, bool OLD>
 __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi) {
   const DevIndex& ix = a.ix;
   const int lane = lane_id();
@@ -774,8 +976,25 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
   w.nb_d = reinterpret_cast<float*>(w.nb_id + a.nbpad);
   w.sk = w.nb_d + a.nbpad;
   w.sv = reinterpret_cast<int*>(w.sk + a.nbpad);
+  w.spare = w.items + a.region_items / 2;
   w.vis = a.visited + (int64_t)slot * a.visited_pitch;
-  w.st_dist = w.st_expand = w.st_greedy = w.st_bytes = 0;
+  w.st_dist = w.st_expand = w.st_greedy = 0;
+  w.st_bytes = 0;
+  w.htab = nullptr;
+  w.hcount = 0;
+  w.spilled = false;
+  char* tail = reinterpret_cast<char*>(w.sv + a.nbpad);
+  if (a.hash_log2 > 0) {
+    const int size = 1 << a.hash_log2;
+    w.htab = reinterpret_cast<int*>(tail);
+    tail += 4 * size;
+    w.hshift = 32 - a.hash_log2;
+    w.hmask = size - 1;
+    w.hlimit = size - size / 4 - 32;
+    for (int t = lane; t < size; t += 32) w.htab[t] = -1;
+    __syncwarp();
+  }
+  w.stage = reinterpret_cast<float*>(tail);
 
   // next epoch of this slot's visited array; clear it when the byte wraps (hnsw.h:582-589)
   int ep = 0;
@@ -798,7 +1017,7 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
   float curdist;
   greedy_descent<R>(a, w, cur, curdist);
   const bool use_old = a.algo == NMSG_ALGO_OLD || (a.algo == NMSG_ALGO_HYBRID && ef >= 1000);
-  if (use_old) {
+  if (OLD && use_old) {
     search_old<R>(a, w, qi, k, ef, cur, curdist, a.old_heap + (int64_t)slot * a.old_heap_cap);
   } else {
     search_v1merge<R>(a, w, qi, k, ef, cur, curdist);
@@ -813,8 +1032,8 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
 }
 
 // Persistent kernel: each warp owns one slot and pulls queries from a work counter.
-template <int R>
-__global__ void __launch_bounds__(128) search_batched_kernel(SearchArgs a) {
+template <int R, bool OLD>
+__global__ void __launch_bounds__(128, 8) search_batched_kernel(SearchArgs a) {
   extern __shared__ __align__(16) char smem[];
   const int warp = threadIdx.x >> 5;
   const int lane = lane_id();
@@ -827,13 +1046,13 @@ __global__ void __launch_bounds__(128) search_batched_kernel(SearchArgs a) {
     item = __shfl_sync(kFull, item, 0);
     if (item >= a.nq) break;
     const int64_t qi = a.order ? a.order[item] : item;
-    run_query<R>(a, wsmem, slot, qi);
+    run_query<R, OLD>(a, wsmem, slot, qi);
   }
 }
 
 // One query per block of one warp; a free slot is taken from the slot locks for the duration.
-template <int R>
-__global__ void __launch_bounds__(32) search_plain_kernel(SearchArgs a) {
+template <int R, bool OLD>
+__global__ void __launch_bounds__(32, 32) search_plain_kernel(SearchArgs a) {
   extern __shared__ __align__(16) char smem[];
   const int lane = lane_id();
   const int64_t qi = blockIdx.x;
@@ -854,50 +1073,65 @@ __global__ void __launch_bounds__(32) search_plain_kernel(SearchArgs a) {
     }
     return;
   }
-  run_query<R>(a, smem, slot, qi);
+  run_query<R, OLD>(a, smem, slot, qi);
   __threadfence();
   if (lane == 0) atomicExch(a.slot_locks + slot, 0);
 }
 
-constexpr int kRowsPerGroup = 2;
-
 }  // namespace
 
-int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad) {
-  int bytes = ix.pitch * 4 + region_items * 8 + nbpad * 16;
+int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int hash_log2, int stage_rows) {
+  int bytes = ix.pitch * 4 + region_items * 8 + nbpad * 16 + (hash_log2 > 0 ? (4 << hash_log2) : 0) +
+              stage_rows * ix.pitch * 4;
   return (bytes + 15) & ~15;
 }
 
-int launch_search_batched(const SearchArgs& a, int blocks, int warps_per_block, void* stream) {
-  const int smem = a.warp_smem * warps_per_block;
-  auto kern = search_batched_kernel<kRowsPerGroup>;
+namespace {
+using Kern = void (*)(SearchArgs);
+
+template <bool OLD>
+Kern pick(bool plain, int gather) {
+  if (plain) {
+    switch (gather) {
+      case 0: return search_plain_kernel<0, OLD>;
+      case 1: return search_plain_kernel<1, OLD>;
+      case 2: return search_plain_kernel<2, OLD>;
+      default: return search_plain_kernel<4, OLD>;
+    }
+  }
+  switch (gather) {
+    case 0: return search_batched_kernel<0, OLD>;
+    case 1: return search_batched_kernel<1, OLD>;
+    case 2: return search_batched_kernel<2, OLD>;
+    default: return search_batched_kernel<4, OLD>;
+  }
+}
+
+Kern kernel_for(bool plain, int gather, bool with_old) {
+  return with_old ? pick<true>(plain, gather) : pick<false>(plain, gather);
+}
+}  // namespace
+
+int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, int blocks, int warps_per_block,
+                  void* stream) {
+  Kern kern = kernel_for(plain, gather, with_old);
+  const int smem = a.warp_smem * (plain ? 1 : warps_per_block);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return (int)e;
-  kern<<<blocks, 32 * warps_per_block, smem, (cudaStream_t)stream>>>(a);
+  if (plain)
+    kern<<<(unsigned)a.nq, 32, smem, (cudaStream_t)stream>>>(a);
+  else
+    kern<<<blocks, 32 * warps_per_block, smem, (cudaStream_t)stream>>>(a);
   return (int)cudaGetLastError();
 }
 
-int launch_search_plain(const SearchArgs& a, void* stream) {
-  auto kern = search_plain_kernel<kRowsPerGroup>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, a.warp_smem);
-  if (e != cudaSuccess) return (int)e;
-  kern<<<(unsigned)a.nq, 32, a.warp_smem, (cudaStream_t)stream>>>(a);
-  return (int)cudaGetLastError();
-}
-
-int occupancy_batched(int warps_per_block, int smem_per_block, int* blocks_per_sm) {
-  auto kern = search_batched_kernel<kRowsPerGroup>;
+int search_occupancy(bool plain, int gather, bool with_old, int warps_per_block, int smem_per_block,
+                     int* blocks_per_sm) {
+  Kern kern = kernel_for(plain, gather, with_old);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_per_block);
   if (e != cudaSuccess) return (int)e;
-  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, 32 * warps_per_block,
+  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, 32 * (plain ? 1 : warps_per_block),
                                                             smem_per_block);
-}
-
-int occupancy_plain(int smem_per_block, int* blocks_per_sm) {
-  auto kern = search_plain_kernel<kRowsPerGroup>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_per_block);
-  if (e != cudaSuccess) return (int)e;
-  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, 32, smem_per_block);
 }
 
 }  // namespace nmsg

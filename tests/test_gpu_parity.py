@@ -131,3 +131,26 @@ def test_zero_query_cosine():
     idx.setQueryTimeParams({"efSearch": 50})
     ids, d = idx.knnQuery(np.zeros(100, np.float32), k=5)
     np.testing.assert_array_equal(d, np.ones(5, np.float32))
+
+
+@pytest.mark.parametrize("cfg", [(4, 1, -1, -1), (2, 4, 8, -1), (1, 2, 10, -1), (4, 4, 14, -1), (4, 0, -1, 16), (2, 0, 9, 3), (1, 0, -1, 64)],
+                         ids=["hbm-visited", "tiny-table-spills", "table-1k", "table-16k", "staged16", "staged3-spill", "staged64"])
+@pytest.mark.parametrize("name,si", [("c1_l2_d128", 0), ("sift_l2_ties", 1), ("sift_l2_ties", 2),
+                                     ("negdot_d960", 2), ("cos_d100", 0), ("dup_l2_d16", 2)])
+def test_launch_shapes_do_not_change_results(name, si, cfg):
+    """Every launch shape (visited set in HBM only, a table small enough to spill mid-query,
+    different rows in flight and warps per block) gives the oracle's results."""
+    k, ef, algo = golden_manifest()[name]["settings"][si]
+    q = load_golden(name)["queries"]
+    idx = _gpu_index(name)
+    idx.setLaunchConfig(*cfg)
+    try:
+        idx.setQueryTimeParams({"efSearch": ef, "algoType": algo})
+        for plain in (False, True):
+            ids, d, cnt, st = idx.knnQueryBatchArrays(q, k, plain=plain, stats=True)
+            oi, od, oc, ost = _oracle(name).search(q, k=k, ef=ef, algo=ALGO_CODES[algo])
+            np.testing.assert_array_equal(ids, oi)
+            np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
+            np.testing.assert_array_equal(st, ost)
+    finally:
+        idx.setLaunchConfig(0, 0, 0)
