@@ -137,6 +137,21 @@ typedef struct nmsg_launch_config {
  * nmsg_knn_batch calls on this handle. Results do not depend on it; speed does. */
 NMSG_API int nmsg_set_launch_config(nmsg_index* index, const nmsg_launch_config* cfg);
 
+/* nmsg_knn_batch for callers that cannot allocate device memory — no counterpart in the
+ * reference (NMSLIB is CPU-only). Some callers must not call cudaMalloc at query time: code
+ * running inside a stream capture that has to stay allocation-free, real-time serving threads
+ * that may not touch the allocator, and processes whose device memory is reserved up front by
+ * another pool. This entry point allocates nothing: queries, ids, dists and counts are caller-
+ * owned DEVICE buffers (row stride kmax), k is uniform and ef/algoType are the handle's, and all
+ * per-call scratch comes from one fixed 32 MiB device array that every GPU loading this library
+ * holds until the process exits. It fails with NMSG_ERR_CAPACITY when the index needs more than
+ * that for even one query slot (one slot needs round_up(n, 16) + 1 bytes, plus
+ * 8 * min(n + 1, 131072) bytes when SearchOld runs). The first call on a device looks up the
+ * array's device address; make it before any stream capture. Calls share the array: calls that
+ * overlap on the GPU race with each other. Returns after the search has finished. */
+NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* index, const float* queries, int64_t nq, int32_t dim, int32_t k,
+                                    int32_t kmax, int32_t* ids, float* dists, int32_t* counts, void* stream);
+
 /* Device status of the last batch on this handle (NMSG_OK or a device-side error code). */
 NMSG_API int nmsg_last_device_status(const nmsg_index* index);
 

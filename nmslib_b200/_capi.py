@@ -65,6 +65,8 @@ def load(path: str = LIB_PATH):
     lib.nmsg_set_query_params.restype = ctypes.c_int
     lib.nmsg_knn_batch.argtypes = [P, P, I64, I32, I32, P, P, I32, P, P, P, P, U32, P]
     lib.nmsg_knn_batch.restype = ctypes.c_int
+    lib.nmsg_knn_batch_noalloc.argtypes = [P, P, I64, I32, I32, I32, P, P, P, P]
+    lib.nmsg_knn_batch_noalloc.restype = ctypes.c_int
     lib.nmsg_set_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
     lib.nmsg_set_launch_config.restype = ctypes.c_int
     lib.nmsg_last_device_status.argtypes = [P]

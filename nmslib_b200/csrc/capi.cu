@@ -10,9 +10,14 @@
 #include <vector>
 
 #include "engine.h"
+#include "handle.h"
 #include "../../include/nmslib_b200.h"
 
 using namespace nmsg;
+
+namespace nmsg {
+void set_last_error(const std::string& msg);
+}
 
 namespace {
 
@@ -34,69 +39,10 @@ int cuda_fail(cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(e_, what); \
   } while (0)
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
-
-// A grow-only device buffer.
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  cudaError_t ensure(size_t want, bool zero) {
-    if (want <= bytes) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-    cudaError_t e = cudaMalloc(&p, want);
-    if (e != cudaSuccess) return e;
-    bytes = want;
-    if (zero) return cudaMemset(p, 0, want);
-    return cudaSuccess;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-  }
-  template <typename T>
-  T* as() const {
-    return reinterpret_cast<T*>(p);
-  }
-};
-
 constexpr int kWarpsPerBlock = 4;
 constexpr int kMaxSmemPerBlock = 227 * 1024;
 
 }  // namespace
-
-struct nmsg_index {
-  int device = 0;
-  int space = 0;
-  int ef = 20;
-  int algo = NMSG_ALGO_HYBRID;
-  int num_sms = 0;
-  HostIndex host;
-  DevIndex dev;
-  DevBuf vecs, l0, up_off, up_links, ext_id;
-  // search scratch (grown on demand)
-  DevBuf visited, epochs, locks, old_heap, counter, status, order, kq, efq;
-  DevBuf q_stage, ids_stage, dists_stage, counts_stage, stats_stage;
-  int slots = 0;            // slots covered by visited/epochs/locks
-  int64_t old_cap = 0;      // entries per slot in old_heap
-  int64_t resident_bytes = 0;
-  int last_status = NMSG_OK;
-  nmsg_launch_config cfg{0, 0, 0, 0};
-  std::mutex mu;
-};
 
 namespace {
 
@@ -164,6 +110,12 @@ int space_matches(int space, int dist_type) {
 extern "C" {
 
 const char* nmsg_last_error(void) { return g_err.c_str(); }
+
+}  // extern "C"
+
+void nmsg::set_last_error(const std::string& msg) { g_err = msg; }
+
+extern "C" {
 
 int nmsg_index_load(const char* path, int space, int device, nmsg_index** out) {
   if (!out || !path) return fail(NMSG_ERR_BAD_ARG, "null argument");
