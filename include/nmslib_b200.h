@@ -60,8 +60,10 @@ enum nmsg_algo { NMSG_ALGO_HYBRID = 0, NMSG_ALGO_OLD = 1, NMSG_ALGO_V1MERGE = 2 
 /* nmsg_knn_batch flags */
 enum nmsg_flags {
   NMSG_DEVICE_PTRS = 1, /* queries and outputs are device pointers; no host copies, no sync */
-  NMSG_PLAIN_KERNEL = 2 /* one query per CUDA block (the unbatched kernel) instead of the
+  NMSG_PLAIN_KERNEL = 2, /* one query per CUDA block (the unbatched kernel) instead of the
                            persistent work-queue kernel */
+  NMSG_CUDA_GRAPH = 4    /* with NMSG_DEVICE_PTRS: launch through a CUDA graph captured on the
+                           first call and replayed while every argument stays the same */
 };
 
 typedef struct nmsg_index_info {
@@ -151,6 +153,43 @@ NMSG_API int nmsg_set_launch_config(nmsg_index* index, const nmsg_launch_config*
  * overlap on the GPU race with each other. Returns after the search has finished. */
 NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* index, const float* queries, int64_t nq, int32_t dim, int32_t k,
                                     int32_t kmax, int32_t* ids, float* dists, int32_t* counts, void* stream);
+
+/* Exact k-NN by scanning every stored vector, the semantics of the reference's sequential
+ * search (similarity_search/src/method/seqsearch.cc:143-177), on the tensor cores: a BF16 GEMM
+ * (FP32 accumulation) keeps candidates per query, an exact rerank in double-float arithmetic
+ * orders them, and a rigorous bound on the BF16 error either certifies the result or triggers a
+ * second pass that collects every vector the bound cannot exclude. The ids are the exact top-k
+ * (ties by id); distances follow the index's space as the HNSW path reports them (squared L2,
+ * 1 - cos on normalised vectors, -dot). dim <= 256, k <= 32. stats (optional, 4 values): queries
+ * certified after the first pass, queries resolved by the second pass, queries whose second-pass
+ * set overflowed (error), base chunks per query block. Buffer conventions as nmsg_knn_batch. */
+NMSG_API int nmsg_bruteforce_knn(nmsg_index* index, const float* queries, int64_t nq, int32_t dim, int32_t k,
+                                 int32_t kmax, int32_t* ids, float* dists, int32_t* counts, int64_t* stats,
+                                 uint32_t flags, void* stream);
+
+/* ---- Serving: continuous batching over a loaded index (no reference counterpart; per-request
+ * semantics are knnQueryBatch's, python_bindings/nmslib.cc:142-168). Requests of 1..max_batch
+ * queries, each with its own k (<= max_k) and efSearch (< 1000, V1Merge), are admitted into
+ * lanes (a stream plus a fixed share of search slots) as lanes free up; the number of lanes is
+ * what memory_budget_bytes allows (at most max_lanes). Requests in different lanes run
+ * concurrently on the device; each request's results do not depend on the others. */
+typedef struct nmsg_server nmsg_server;
+
+NMSG_API int nmsg_server_create(nmsg_index* index, int64_t memory_budget_bytes, int32_t max_batch, int32_t max_k,
+                                int32_t max_lanes, nmsg_server** out);
+NMSG_API int nmsg_server_lanes(const nmsg_server* server);
+/* Copies the queries; returns at once with a request id. */
+NMSG_API int nmsg_server_submit(nmsg_server* server, const float* queries, int32_t nq, int32_t k, int32_t ef,
+                                int64_t* request_id);
+/* Blocks until the request finished; ids/dists are nq x k, counts nq; latency from submission. */
+NMSG_API int nmsg_server_wait(nmsg_server* server, int64_t request_id, int32_t* ids, float* dists, int32_t* counts,
+                              double* latency_s);
+/* Open-loop replay of a request trace (arrival times in seconds from the start); per-request
+ * latency from the scheduled arrival to completion, and the wall time of the whole trace. */
+NMSG_API int nmsg_server_run_trace(nmsg_server* server, const float* queries, const int64_t* q_offset,
+                                   const int32_t* nq, const int32_t* k, const int32_t* ef, const double* arrival_s,
+                                   int64_t nreq, double* latency_s, double* wall_s);
+NMSG_API void nmsg_server_free(nmsg_server* server);
 
 /* Device status of the last batch on this handle (NMSG_OK or a device-side error code). */
 NMSG_API int nmsg_last_device_status(const nmsg_index* index);

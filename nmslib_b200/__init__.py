@@ -255,6 +255,22 @@ class FloatIndex:
                                                 flags, None))
         return (ids, dists, counts, st) if stats else (ids, dists, counts)
 
+    def bruteForceBatchArrays(self, queries, k=10, stats=False):
+        """Exact k-NN over every stored vector (seq_search semantics) on the tensor cores:
+        (ids [nq, k] external, dists [nq, k], counts [nq][, stats [4]]). k <= 32, dim <= 256."""
+        h = self._require()
+        q = self._queries(queries)
+        nq = q.shape[0]
+        ids = np.empty((nq, k), np.int32)
+        dists = np.empty((nq, k), np.float32)
+        counts = np.empty(nq, np.int32)
+        st = np.zeros(4, np.int64)
+        ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        dim = q.shape[1] if nq else (self._info.dim if self._info else 0)
+        _capi.check(_capi.load().nmsg_bruteforce_knn(h, ptr(q), nq, dim, int(k), int(k), ptr(ids), ptr(dists),
+                                                     ptr(counts), ptr(st), 0, None))
+        return (ids, dists, counts, st) if stats else (ids, dists, counts)
+
     def knnQueryBatch(self, queries, k=10, num_threads=0):
         """IndexWrapper::knnQueryBatch (nmslib.cc:142-168): a list of (ids int32[], dists float32[])
         per query, ascending distance. num_threads is accepted for compatibility and unused."""

@@ -19,7 +19,7 @@ ERR_DEVICE, ERR_TIMEOUT, ERR_CORRUPT_GRAPH, ERR_CAPACITY = -5, -6, -7, -8
 
 SPACE_L2, SPACE_COSINE, SPACE_NEGDOT = 0, 1, 2
 ALGO_HYBRID, ALGO_OLD, ALGO_V1MERGE = 0, 1, 2
-FLAG_DEVICE_PTRS, FLAG_PLAIN_KERNEL = 1, 2
+FLAG_DEVICE_PTRS, FLAG_PLAIN_KERNEL, FLAG_CUDA_GRAPH = 1, 2, 4
 
 
 class IndexInfo(ctypes.Structure):
@@ -67,6 +67,20 @@ def load(path: str = LIB_PATH):
     lib.nmsg_knn_batch.restype = ctypes.c_int
     lib.nmsg_knn_batch_noalloc.argtypes = [P, P, I64, I32, I32, I32, P, P, P, P]
     lib.nmsg_knn_batch_noalloc.restype = ctypes.c_int
+    lib.nmsg_bruteforce_knn.argtypes = [P, P, I64, I32, I32, I32, P, P, P, P, U32, P]
+    lib.nmsg_bruteforce_knn.restype = ctypes.c_int
+    lib.nmsg_server_create.argtypes = [P, I64, I32, I32, I32, ctypes.POINTER(P)]
+    lib.nmsg_server_create.restype = ctypes.c_int
+    lib.nmsg_server_lanes.argtypes = [P]
+    lib.nmsg_server_lanes.restype = ctypes.c_int
+    lib.nmsg_server_submit.argtypes = [P, P, I32, I32, I32, ctypes.POINTER(ctypes.c_int64)]
+    lib.nmsg_server_submit.restype = ctypes.c_int
+    lib.nmsg_server_wait.argtypes = [P, I64, P, P, P, ctypes.POINTER(ctypes.c_double)]
+    lib.nmsg_server_wait.restype = ctypes.c_int
+    lib.nmsg_server_run_trace.argtypes = [P, P, P, P, P, P, P, I64, P, ctypes.POINTER(ctypes.c_double)]
+    lib.nmsg_server_run_trace.restype = ctypes.c_int
+    lib.nmsg_server_free.argtypes = [P]
+    lib.nmsg_server_free.restype = None
     lib.nmsg_set_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
     lib.nmsg_set_launch_config.restype = ctypes.c_int
     lib.nmsg_last_device_status.argtypes = [P]

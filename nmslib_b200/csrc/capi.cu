@@ -39,8 +39,6 @@ int cuda_fail(cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(e_, what); \
   } while (0)
 
-constexpr int kWarpsPerBlock = 4;
-constexpr int kMaxSmemPerBlock = 227 * 1024;
 
 }  // namespace
 
@@ -107,6 +105,54 @@ int space_matches(int space, int dist_type) {
 
 }  // namespace
 
+namespace nmsg {
+
+int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bool with_old, bool plain,
+                LaunchPlan* out, std::string* err) {
+  LaunchPlan p;
+  p.with_old = with_old;
+  p.nbpad = ((std::max(d.maxM, d.maxM0) + 1 + 31) / 32) * 32;
+  p.region = (region + 1) & ~1;  // keeps the following shared-memory pieces 16-byte aligned
+  // Launch shape: explicit configuration, else defaults by vector width and beam size.
+  // Measured on B200 (1M x 128 SIFT-like, 10K queries, k 10): staging rows through shared memory
+  // beats register gathers at every beam size; 8 rows per round is best up to efSearch 128
+  // (4.10M q/s at 64 vs 3.47M for two register rows per 8-lane group), 4 rows at efSearch 256
+  // (1.90M vs 1.64M), where the larger beam array leaves less shared memory per warp.
+  p.stage_rows = 0;
+  if (cfg.stage_rows > 0) {
+    p.gather = 0;
+    p.stage_rows = cfg.stage_rows;
+  } else if (cfg.stage_rows == 0 && cfg.rows_per_group == 0 && d.pitch <= 256) {
+    p.gather = 0;
+    p.stage_rows = p.region <= 160 ? 8 : 4;
+  } else {
+    p.gather = cfg.rows_per_group ? cfg.rows_per_group : (d.pitch <= 256 ? 2 : 1);
+  }
+  const int hl = cfg.visited_hash_log2 == 0 ? -1 : cfg.visited_hash_log2;  // default: visited set in HBM
+  p.hash_log2 = hl > 0 ? hl : 0;
+  p.warp_smem = warp_smem_bytes(d, p.region, p.nbpad, p.hash_log2, p.stage_rows);
+  while (p.gather == 0 && p.stage_rows > 1 && p.warp_smem > kMaxSmemPerBlock) {  // wide rows: fewer per round
+    p.stage_rows = (p.stage_rows + 1) / 2;
+    p.warp_smem = warp_smem_bytes(d, p.region, p.nbpad, p.hash_log2, p.stage_rows);
+  }
+  p.wpb = plain ? 1 : (cfg.warps_per_block ? cfg.warps_per_block : kWarpsPerBlock);
+  while (p.wpb > 1 && p.wpb * p.warp_smem > kMaxSmemPerBlock) p.wpb >>= 1;
+  if (p.wpb * p.warp_smem > kMaxSmemPerBlock) {
+    *err = "max(ef, k) = " + std::to_string(p.region) + " needs more shared memory per query than a block has";
+    return NMSG_ERR_CAPACITY;
+  }
+  p.blocks_per_sm = 0;
+  const int rc = search_occupancy(plain, p.gather, with_old, p.wpb, p.wpb * p.warp_smem, &p.blocks_per_sm);
+  if (rc != 0 || p.blocks_per_sm < 1) {
+    *err = "no resident block fits this configuration";
+    return NMSG_ERR_DEVICE;
+  }
+  *out = p;
+  return NMSG_OK;
+}
+
+}  // namespace nmsg
+
 extern "C" {
 
 const char* nmsg_last_error(void) { return g_err.c_str(); }
@@ -170,6 +216,9 @@ void nmsg_index_free(nmsg_index* h) {
   if (!h) return;
   {
     DeviceGuard g(h->device);
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    destroy_bruteforce(h->bf);
+    h->bf = nullptr;
     for (DevBuf* b : {&h->vecs, &h->l0, &h->up_off, &h->up_links, &h->ext_id, &h->visited, &h->epochs, &h->locks,
                       &h->old_heap, &h->counter, &h->status, &h->order, &h->kq, &h->efq, &h->q_stage,
                       &h->ids_stage, &h->dists_stage, &h->counts_stage, &h->stats_stage})
@@ -245,9 +294,9 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
     if (eq < 0) return fail(NMSG_ERR_BAD_ARG, "ef must be non-negative");
     const bool old = algo == NMSG_ALGO_OLD || (algo == NMSG_ALGO_HYBRID && eq >= 1000);
     any_old |= old;
-    // V1Merge keeps its sorted array twice (merge target); SearchOld keeps its closest-set heap
-    // (ef + 1) and the k results
-    region = std::max(region, old ? eq + 1 + kq : 2 * std::max(eq, kq));
+    // V1Merge keeps its sorted array of max(ef, k) items; SearchOld its closest-set heap (ef + 1)
+    // and the k results
+    region = std::max(region, old ? eq + 1 + kq : std::max(eq, kq));
     if (!k_per_q && !ef_per_q) break;  // uniform batch: one check covers every query
   }
   if (nq == 0) return NMSG_OK;
@@ -273,48 +322,23 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
   const bool plain = flags & NMSG_PLAIN_KERNEL;
 
   SearchArgs a;
+  std::memset(&a, 0, sizeof(a));  // padding too: the CUDA-graph cache compares argument bytes
   a.ix = d;
   a.nq = nq;
   a.k_default = k;
   a.ef_default = ef;
   a.algo = algo;
   a.kmax = kmax;
-  a.nbpad = ((std::max(d.maxM, d.maxM0) + 1 + 31) / 32) * 32;
-  region = (region + 1) & ~1;  // keeps the following shared-memory pieces 16-byte aligned
-  a.region_items = region;
-  // launch shape: explicit configuration, else defaults by vector width and beam size
-  // Measured on B200 (1M x 128, 10K queries): staging 8 rows per round through shared memory is
-  // fastest for small beams (efSearch 64: 4.4M q/s vs 3.7M with register gathers), two rows per
-  // 8-lane group in registers for large ones (efSearch 256: 1.71M vs 1.67M).
-  int gather, stage_rows = 0;
-  const int beam = region / 2;
-  if (h->cfg.stage_rows > 0) {
-    gather = 0;
-    stage_rows = h->cfg.stage_rows;
-  } else if (h->cfg.stage_rows == 0 && h->cfg.rows_per_group == 0 && beam <= 160 && d.pitch <= 256) {
-    gather = 0;
-    stage_rows = 8;
-  } else {
-    gather = h->cfg.rows_per_group ? h->cfg.rows_per_group : (d.pitch <= 256 ? 2 : 1);
-  }
-  int hl = h->cfg.visited_hash_log2;
-  if (hl == 0) hl = -1;  // default: visited set in HBM (measured fastest at the default shapes)
-  a.hash_log2 = hl > 0 ? hl : 0;
-  a.stage_rows = stage_rows;
-  a.warp_smem = warp_smem_bytes(d, region, a.nbpad, a.hash_log2, stage_rows);
-  while (gather == 0 && stage_rows > 1 && a.warp_smem > kMaxSmemPerBlock) {  // wide rows: fewer per round
-    stage_rows = (stage_rows + 1) / 2;
-    a.stage_rows = stage_rows;
-    a.warp_smem = warp_smem_bytes(d, region, a.nbpad, a.hash_log2, stage_rows);
-  }
-  int wpb = plain ? 1 : (h->cfg.warps_per_block ? h->cfg.warps_per_block : kWarpsPerBlock);
-  while (wpb > 1 && wpb * a.warp_smem > kMaxSmemPerBlock) wpb >>= 1;
-  if (wpb * a.warp_smem > kMaxSmemPerBlock)
-    return fail(NMSG_ERR_CAPACITY, "max(ef, k) = " + std::to_string(region / 2) +
-                                       " needs more shared memory per query than a block has");
-  int bps = 0;
-  int rc = search_occupancy(plain, gather, any_old, wpb, wpb * a.warp_smem, &bps);
-  if (rc != 0 || bps < 1) return fail(NMSG_ERR_DEVICE, "no resident block fits this configuration");
+  LaunchPlan plan;
+  std::string perr;
+  int rc = plan_launch(d, h->cfg, region, any_old, plain, &plan, &perr);
+  if (rc != NMSG_OK) return fail(rc, perr);
+  region = plan.region;
+  a.region_items = plan.region;
+  a.hash_log2 = plan.hash_log2;
+  a.stage_rows = plan.stage_rows;
+  a.warp_smem = plan.warp_smem;
+  const int gather = plan.gather, wpb = plan.wpb, bps = plan.blocks_per_sm;
   const int blocks = plain ? 0 : bps * h->num_sms;
   const int slots = plain ? bps * h->num_sms : blocks * wpb;
   // scratch
@@ -385,6 +409,39 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
       NMSG_CUDA(cudaMemcpy(h->order.p, order.data(), nq * 4, cudaMemcpyHostToDevice), "copy order");
       a.order = h->order.as<int32_t>();
     }
+  }
+  a.nbpad = plan.nbpad;
+  if (dev_ptrs && (flags & NMSG_CUDA_GRAPH)) {
+    // Replay the captured launch when every argument is the same as last time; otherwise
+    // capture (counter and status resets + kernel) into a new graph.
+    const bool same = h->graph_exec && std::memcmp(&h->graph_args, &a, sizeof(SearchArgs)) == 0 &&
+                      h->graph_shape[0] == (int)plain && h->graph_shape[1] == gather &&
+                      h->graph_shape[2] == (int)any_old && h->graph_shape[3] == blocks && h->graph_shape[4] == wpb;
+    if (!same) {
+      if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+      h->graph_exec = nullptr;
+      NMSG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+      cudaMemsetAsync(a.work_counter, 0, 4, st);
+      cudaMemsetAsync(a.status, 0, 4, st);
+      const int lrc = launch_search(a, plain, gather, any_old, blocks, wpb, stream);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+      if (lrc != 0 || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_fail(ce != cudaSuccess ? ce : (cudaError_t)lrc, "capture search launch");
+      }
+      const cudaError_t ie = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) return cuda_fail(ie, "instantiate search graph");
+      std::memcpy(&h->graph_args, &a, sizeof(SearchArgs));
+      h->graph_shape[0] = (int)plain;
+      h->graph_shape[1] = gather;
+      h->graph_shape[2] = (int)any_old;
+      h->graph_shape[3] = blocks;
+      h->graph_shape[4] = wpb;
+    }
+    NMSG_CUDA(cudaGraphLaunch(h->graph_exec, st), "graph launch");
+    return NMSG_OK;
   }
   NMSG_CUDA(cudaMemsetAsync(a.work_counter, 0, 4, st), "reset counter");
   NMSG_CUDA(cudaMemsetAsync(a.status, 0, 4, st), "reset status");

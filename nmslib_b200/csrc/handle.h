@@ -12,8 +12,32 @@
 
 namespace nmsg {
 
+struct BruteForceState;  // bruteforce.cu
+void destroy_bruteforce(BruteForceState* s);
+
 // Sets the thread-local message returned by nmsg_last_error().
 void set_last_error(const std::string& msg);
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kMaxSmemPerBlock = 227 * 1024;
+
+// Launch shape of one search launch (see plan_launch).
+struct LaunchPlan {
+  int gather = 1;         // 0: staged rows in shared memory; 1/2/4: register rows per 8-lane group
+  int stage_rows = 0;
+  int hash_log2 = 0;
+  int region = 0;         // shared-memory items per warp (beam array or SearchOld heaps)
+  int nbpad = 32;
+  int warp_smem = 0;
+  int wpb = kWarpsPerBlock;
+  int blocks_per_sm = 0;
+  bool with_old = false;
+};
+
+// Chooses gather mode, shared-memory sizes and warps per block for a launch whose largest query
+// needs `region` items, honouring explicit settings in cfg; returns an nmsg_status.
+int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bool with_old, bool plain,
+                LaunchPlan* out, std::string* err);
 
 struct DeviceGuard {
   int prev = -1;
@@ -73,5 +97,9 @@ struct nmsg_index {
   int64_t resident_bytes = 0;
   int last_status = NMSG_OK;
   nmsg_launch_config cfg{0, 0, 0, 0};
+  nmsg::BruteForceState* bf = nullptr;  // brute-force data, built on first use
+  cudaGraphExec_t graph_exec = nullptr;  // last captured device-pointer search (NMSG_CUDA_GRAPH)
+  nmsg::SearchArgs graph_args{};
+  int graph_shape[5] = {0, 0, 0, 0, 0};
   std::mutex mu;
 };

@@ -463,19 +463,33 @@ __device__ int sorted_insert(uint2* items, int& num, int cap, float key, int id)
   return pos;
 }
 
-// Inserts a sorted batch sk/sv[0..m) into items[0..num) in one parallel pass, writing the result
-// to `spare`. Exact only when no key of the batch equals another batch key or a key already in
-// the array: then push_or_replace_non_empty_exp always lands on the lower bound, so sequential
-// insertion equals a stable merge truncated to `cap`, and the smallest returned insertion index is
-// the merged position of the first batch item. Returns false (nothing changed) when a tie exists.
-__device__ bool merge_batch(const uint2* items, uint2* spare, int num, int cap, const float* sk, const int* sv,
-                            int m, int* first_pos) {
+// Inserts the batch sk/sv[0..m) (in list order, not yet sorted) into items[0..num) in one
+// parallel pass, in place. Exact only when no key of the batch equals another batch key or a key
+// already in the array: then push_or_replace_non_empty_exp always lands on the lower bound, so
+// sorting the batch and inserting it item by item equals a stable merge truncated to `cap`, and
+// the smallest insertion index is the merged position of the smallest batch item. Every item's
+// merged position is its lower bound in the array plus its rank in the batch; array items from
+// the first insertion point on move right by the number of batch keys below them (processed
+// from the tail, so nothing is overwritten before it is read). Returns false, with nothing
+// changed, when a tie exists.
+__device__ bool merge_unsorted_batch(uint2* items, int& num, int cap, const float* sk, const int* sv, int m,
+                                     float* tk, int* tv, int* first_pos) {
   const int lane = lane_id();
   bool tie = false;
-  int p0 = cap;
-  for (int i = lane; i < m; i += 32) {
+  int pmin = 0x7fffffff;
+  int rk[4];  // m <= nbpad <= 128: ranks of this lane's items
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = lane + 32 * r;
+    if (i >= m) break;
     const float key = sk[i];
-    if (i + 1 < m && sk[i + 1] == key) tie = true;
+    int rank = 0;
+    for (int u = 0; u < m; ++u) {
+      const float ku = sk[u];
+      rank += ku < key;
+      tie |= (ku == key) && (u != i);
+    }
+    rk[r] = rank;
     int lo = 0, hi = num;
     while (lo < hi) {
       const int mid = (lo + hi) >> 1;
@@ -484,30 +498,52 @@ __device__ bool merge_batch(const uint2* items, uint2* spare, int num, int cap, 
       else
         hi = mid;
     }
-    if (lo < num && key_of(items[lo]) == key) tie = true;
-    const int p = lo + i;
-    if (i == 0) p0 = p;
-    if (p < cap) spare[p] = make_item(key, sv[i], false);
+    tie |= lo < num && key_of(items[lo]) == key;
+    tk[rank] = key;  // the batch in sorted order (ranks are distinct when there is no tie)
+    tv[rank] = lo;   // and each item's lower bound in the array
+    pmin = min(pmin, lo + rank);
   }
   if (__any_sync(kFull, tie)) {
     __syncwarp();
     return false;
   }
-  for (int t = lane; t < num; t += 32) {
-    const uint2 it = items[t];
-    const float key = key_of(it);
-    int lo = 0, hi = m;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (sk[mid] < key)
-        lo = mid + 1;
-      else
-        hi = mid;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pmin = min(pmin, __shfl_xor_sync(kFull, pmin, o));
+  __syncwarp();
+  // shift the array tail [p0, num): each item moves right by the count of batch keys below it
+  // (binary search over the sorted batch), from the tail so nothing is overwritten before it is read
+  const int p0 = min(pmin, num);
+  for (int hi = num; hi > p0; hi -= 32) {
+    const int t = hi - 1 - lane;
+    const bool act = t >= p0;
+    uint2 it;
+    int dst = cap;
+    if (act) {
+      it = items[t];
+      const float key = key_of(it);
+      int lo = 0, h2 = m;
+      while (lo < h2) {
+        const int mid = (lo + h2) >> 1;
+        if (tk[mid] < key)
+          lo = mid + 1;
+        else
+          h2 = mid;
+      }
+      dst = t + lo;
     }
-    const int p = t + lo;
-    if (p < cap) spare[p] = it;
+    __syncwarp();
+    if (act && dst < cap) items[dst] = it;
+    __syncwarp();
   }
-  *first_pos = __shfl_sync(kFull, p0, 0);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = lane + 32 * r;
+    if (i >= m) break;
+    const int p = tv[rk[r]] + rk[r];
+    if (p < cap) items[p] = make_item(sk[i], sv[i], false);
+  }
+  num = min(num + m, cap);
+  *first_pos = pmin;
   __syncwarp();
   return true;
 }
@@ -581,7 +617,6 @@ struct WarpCtx {
   float* nb_d;   // [nbpad]
   float* sk;     // [nbpad]
   int* sv;       // [nbpad]
-  uint2* spare;  // V1Merge: second buffer of the sorted array (merge target)
   float* stage;  // staged-gather rows (stage_rows x pitch), or null
   int* htab;     // shared-memory visited table (open addressing, -1 = empty), or null
   uint8_t* vis;  // HBM epoch bytes of this warp's slot
@@ -818,7 +853,6 @@ __device__ void search_v1merge(const SearchArgs& a, WarpCtx& w, int64_t qi, int 
   const int lane = lane_id();
   const int cap = max(ef, k);
   uint2* items = w.items;
-  uint2* spare = w.spare;
   int num = 1;
   if (lane == 0) items[0] = make_item(curdist, cur, false);
   visit_one(w, cur);
@@ -868,15 +902,11 @@ __device__ void search_v1merge(const SearchArgs& a, WarpCtx& w, int64_t qi, int 
     }
     __syncwarp();
     if (qty) {
-      sort_like_std(w.sk, w.sv, qty, w.nb_d, w.nb_id);
       int p0;
-      if (merge_batch(items, spare, num, cap, w.sk, w.sv, qty, &p0)) {
-        uint2* t = items;
-        items = spare;
-        spare = t;
-        num = min(num + qty, cap);
+      if (merge_unsorted_batch(items, num, cap, w.sk, w.sv, qty, w.nb_d, w.nb_id, &p0)) {
         if (p0 < curr) curr = p0;
       } else {
+        sort_like_std(w.sk, w.sv, qty, w.nb_d, w.nb_id);
         for (int i = 0; i < qty; ++i) {
           const int ins = sorted_insert(items, num, cap, w.sk[i], w.sv[i]);
           if (ins < curr) curr = ins;
@@ -976,7 +1006,6 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
   w.nb_d = reinterpret_cast<float*>(w.nb_id + a.nbpad);
   w.sk = w.nb_d + a.nbpad;
   w.sv = reinterpret_cast<int*>(w.sk + a.nbpad);
-  w.spare = w.items + a.region_items / 2;
   w.vis = a.visited + (int64_t)slot * a.visited_pitch;
   w.st_dist = w.st_expand = w.st_greedy = 0;
   w.st_bytes = 0;

@@ -116,7 +116,7 @@ extern "C" NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* h, const float* queri
   a.dists = dists;
   a.counts = counts;
   a.nbpad = ((std::max(d.maxM, d.maxM0) + 1 + 31) / 32) * 32;
-  a.region_items = ((old ? ef + 1 + k : 2 * std::max(ef, k)) + 1) & ~1;
+  a.region_items = ((old ? ef + 1 + k : std::max(ef, k)) + 1) & ~1;
   a.hash_log2 = 0;
   a.stage_rows = 0;
   const int gather = d.pitch <= 256 ? 2 : 1;

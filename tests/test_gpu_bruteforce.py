@@ -1,0 +1,85 @@
+"""The tensor-core brute-force k-NN against an exact float64 scan of the same stored vectors:
+identical ids (ties by id) and distances within float rounding."""
+import numpy as np
+import pytest
+
+import nmslib_b200 as nmslib
+from nmslib_b200 import _capi
+from nmslib_b200.build import build
+from oracle.oracle import OracleIndex, normalize
+
+from conftest import golden_manifest, golden_path, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def fp64_topk(name_or_path, queries, k, space):
+    """Exact top-k over the index's stored vectors in float64: keys q.x (cosine: the query
+    normalised as the engine normalises it; negdot) or 2 q.x - |x|^2 (l2); ties by node index."""
+    ix = OracleIndex(name_or_path)
+    vecs, ext, _, _ = ix.export()
+    x = vecs.astype(np.float64)
+    out_i, out_d = [], []
+    for q in queries:
+        qf = normalize(q) if space == "cosinesimil" else np.asarray(q, np.float32)
+        qd = qf.astype(np.float64)
+        dot = x @ qd
+        key = 2 * dot - (x * x).sum(1) if space == "l2" else dot
+        order = np.lexsort((np.arange(len(key)), -key))[:k]
+        out_i.append(ext[order])
+        if space == "l2":
+            out_d.append((qd @ qd) - key[order])
+        elif space == "cosinesimil":
+            out_d.append(np.maximum(0, 1 - np.clip(key[order], -1, 1)))
+        else:
+            out_d.append(-key[order])
+    return np.array(out_i), np.array(out_d)
+
+
+def _index(name):
+    build()
+    idx = nmslib.init(method="hnsw", space=golden_manifest()[name]["space"])
+    idx.loadIndex(golden_path(name))
+    return idx
+
+
+@pytest.mark.parametrize("name,k", [("tiny_l2_d20_sqids", 10), ("one_l2_d3", 3), ("tiny_cos_d48", 7),
+                                    ("dup_l2_d16", 10), ("c1_l2_d128", 10), ("c1_l2_d128", 32),
+                                    ("cos_d100", 10), ("cos_d100", 1), ("sift_l2_ties", 10),
+                                    ("tiny_negdot_d7", 5)])
+def test_bruteforce_matches_fp64(name, k):
+    space = golden_manifest()[name]["space"]
+    idx = _index(name)
+    q = load_golden(name)["queries"]
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True)
+    n = idx.info["n"]
+    want_i, want_d = fp64_topk(golden_path(name), q, min(k, n), space)
+    np.testing.assert_array_equal(cnt, np.full(len(q), min(k, n)))
+    np.testing.assert_array_equal(ids[:, : min(k, n)], want_i)
+    np.testing.assert_allclose(d[:, : min(k, n)], want_d, rtol=2e-6, atol=2e-6)
+    assert st[0] + st[1] == len(q) and st[2] == 0
+
+
+def test_bruteforce_limits():
+    idx = _index("negdot_d960")
+    q = load_golden("negdot_d960")["queries"][:4]
+    with pytest.raises(RuntimeError, match="dim <= 256"):
+        idx.bruteForceBatchArrays(q, 10)
+    idx = _index("c1_l2_d128")
+    with pytest.raises(RuntimeError, match="k <= 32"):
+        idx.bruteForceBatchArrays(load_golden("c1_l2_d128")["queries"][:4], 33)
+
+
+def test_bruteforce_larger_cosine(tmp_path):
+    """200K x 100 cosine (the C3 distribution): exact ids against float64 on a sample."""
+    from nmslib_b200.datasets import mixture
+    x = mixture("glove", 200_256, 100, 100, 3)
+    base, q = x[:200_000], x[200_000:]
+    p = str(tmp_path / "c3s.hnsw")
+    _capi.build_index(base, 1, 8, 40, nthreads=0, out_path=p)
+    idx = nmslib.init(method="hnsw", space="cosinesimil")
+    idx.loadIndex(p)
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, 10, stats=True)
+    want_i, want_d = fp64_topk(p, q, 10, "cosinesimil")
+    np.testing.assert_array_equal(ids, want_i)
+    np.testing.assert_allclose(d, want_d, rtol=2e-6, atol=2e-6)
