@@ -232,6 +232,175 @@ def cpu_reference_qps(path, queries, ef, k, target_seconds=3.0, space="l2"):
     return n / best, n, kind, cores
 
 
+# ------------------------------------------------------------------ serving and brute force
+def serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6), seconds=1.0, seed=11):
+    """p50/p99 request latency and achieved QPS of the continuous-batching server at several
+    offered loads (queries per second), open-loop Poisson arrivals."""
+    from nmslib_b200.serving import Server
+    rng = np.random.default_rng(seed)
+    srv = Server(index, memory_budget_bytes=8 << 30, max_batch=256, max_k=100, max_lanes=32)
+    out = []
+    try:
+        for qps in rates_qps:
+            mean_batch = (256 - 1) / np.log(256)
+            n_req = int(qps * seconds / mean_batch)
+            sizes = np.minimum(256, np.floor(np.exp(rng.uniform(0, np.log(257), n_req)))).astype(np.int32)
+            ks = rng.choice([10, 100], n_req).astype(np.int32)
+            efs = rng.choice([100, 400], n_req).astype(np.int32)
+            offs = rng.integers(0, len(queries) - 256, n_req)
+            arrivals = np.cumsum(rng.exponential(mean_batch / qps, n_req))
+            lat, wall = srv.run_trace(queries, offs, sizes, ks, efs, arrivals)
+            small = sizes <= 256
+            out.append({"offered_qps": qps, "requests": n_req, "achieved_qps": round(float(sizes.sum()) / wall),
+                        "p50_ms": round(float(np.percentile(lat[small], 50)) * 1e3, 3),
+                        "p99_ms": round(float(np.percentile(lat[small], 99)) * 1e3, 3), "lanes": srv.lanes})
+            log(f"[bench] serving {qps:.0f} q/s offered: {out[-1]}")
+    finally:
+        srv.close()
+    return {"workload": WORKLOAD + " index, request mix of the 5M serving config", "points": out}
+
+
+def brute_force_measure(index, queries, k=10, reps=3):
+    """Exact k-NN of the whole batch over every stored vector (tcgen05 BF16 GEMM + exact rerank):
+    time and tensor throughput (2 * nq * n * padded dim FLOP per batch)."""
+    import torch
+    ids, d, c, st = index.bruteForceBatchArrays(queries, k, stats=True)  # builds the BF16 copy
+    t = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        index.bruteForceBatchArrays(queries, k)
+        t.append(time.perf_counter() - t0)
+    best = min(t)
+    n, dim = index.info["n"], index.info["dim"]
+    kp = (dim + 63) // 64 * 64
+    flops = 2.0 * len(queries) * n * kp
+    res = {"queries": len(queries), "k": k, "ms_end_to_end": round(best * 1e3, 3),
+           "qps": round(len(queries) / best), "tensor_tflops": round(flops / best / 1e12, 1),
+           "certified_first_pass": int(st[0]), "second_pass": int(st[1]), "overflow": int(st[2])}
+    log(f"[bench] brute force: {res}")
+    return res
+
+
+# ------------------------------------------------------------------ the other workloads
+AUX = {"c3": "c3_glove1m_d100_cos", "c4": "c4_abs1m_d960_negdot", "c5": "c5_unit5m_d96_l2"}
+
+
+def fp64_truth(base, queries, k, space):
+    """Exact float64 top-k keys on the GPU (measurement only): k-th best distance per query."""
+    import torch
+    b = torch.from_numpy(base).cuda().double()
+    if space == "cosinesimil":
+        b = b / b.norm(dim=1, keepdim=True).clamp_min(1e-300)
+    bsq = (b * b).sum(1)
+    kth = np.empty(len(queries))
+    for s0 in range(0, len(queries), 256):
+        q = torch.from_numpy(queries[s0:s0 + 256]).cuda().double()
+        if space == "cosinesimil":
+            q = q / q.norm(dim=1, keepdim=True).clamp_min(1e-300)
+            d = 1 - q @ b.T
+        elif space == "negdotprod":
+            d = -(q @ b.T)
+        else:
+            d = (q * q).sum(1, keepdim=True) - 2 * q @ b.T + bsq[None, :]
+        v, _ = torch.topk(d, k, dim=1, largest=False)
+        kth[s0:s0 + 256] = v[:, -1].cpu().numpy()
+    del b
+    torch.cuda.empty_cache()
+    return kth
+
+
+def run_aux(args):
+    import torch
+
+    import nmslib_b200 as nmslib
+    from nmslib_b200 import SPACES, _capi
+    from nmslib_b200.build import build
+    from nmslib_b200.datasets import workload
+    build()
+    name = AUX[args.workload]
+    base, queries, space, m = workload(name)
+    path = os.path.join(CACHE_DIR, f"{name}_M{m}_efc{EFC}_seed0.hnsw")
+    if not os.path.exists(path):
+        os.makedirs(CACHE_DIR, exist_ok=True)
+        t0 = time.time()
+        _capi.build_index(base, SPACES[space], m, EFC, nthreads=0, seed=0, out_path=path + ".tmp")
+        os.replace(path + ".tmp", path)
+        log(f"[bench] built {path} in {time.time() - t0:.1f}s")
+    index = nmslib.init(method="hnsw", space=space)
+    index.loadIndex(path)
+    out = {"workload": name, "n_base": len(base), "nq": len(queries), "dim": base.shape[1], "M": m,
+           "efConstruction": EFC, "space": space}
+
+    def timed(fn, reps=3):
+        fn()
+        best = None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = fn()
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        return best, r
+
+    if args.workload in ("c3", "c5"):
+        qs = queries[:10_000]
+        kth = fp64_truth(base, qs, 10, space)
+        rows = []
+        for ef in ((50, 100, 200, 400) if args.workload == "c3" else (50, 100, 200, 400)):
+            index.setQueryTimeParams({"efSearch": ef})
+            dt, (ids, d, cnt) = timed(lambda: index.knnQueryBatchArrays(qs, 10))
+            rows.append({"efSearch": ef, "recall@10": round(recall_at_k(d.astype(np.float64), cnt, kth, 10), 4),
+                         "qps_e2e": round(len(qs) / dt)})
+            log(f"[bench] {name} ef={ef}: {rows[-1]}")
+        out["hnsw"] = rows
+        ef_ref = 200 if args.workload == "c3" else 100
+        qps, n, kind, cores = cpu_reference_qps(path, qs, ef_ref, 10, space=space)
+        out["cpu_reference"] = {"efSearch": ef_ref, "qps": round(qps), "cores": cores, "kind": kind, "sample": n}
+    if args.workload == "c3":
+        out["bruteforce"] = brute_force_measure(index, queries[:10_000])
+    if args.workload == "c5":
+        out["serving"] = serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6, 2e6))
+    if args.workload == "c4":
+        rng = np.random.default_rng(4)
+        nq = len(queries)
+        k = rng.choice([1, 10, 100], nq).astype(np.int32)
+        ef = rng.integers(64, 1025, nq).astype(np.int32)
+        kth = fp64_truth(base, queries, 100, space)
+        dt, (ids, d, cnt) = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
+        # recall@k per query against the float64 k-th distance of that query's own k
+        kth_k = np.array([fp for fp in kth])  # k = 100 column; per-k recall below uses the row's own k
+        out["mixed_batch"] = {"queries": nq, "qps_e2e": round(nq / dt), "ms": round(dt * 1e3, 2),
+                              "searchold_queries": int((ef >= 1000).sum())}
+        truth10 = fp64_truth(base, queries, 10, space)
+        sel = k == 10
+        out["mixed_batch"]["recall@10_of_k10_queries"] = round(
+            recall_at_k(d[sel][:, :10].astype(np.float64), cnt[sel], truth10[sel], 10), 4)
+        del kth_k
+        # reference: the same mixed batch, grouped by (k, ef) as the reference needs one ef per call
+        ref = reference_module_or_none()
+        if ref is not None:
+            idx = ref.init(method="hnsw", space=space)
+            idx.loadIndex(path)
+            sample = np.arange(min(nq, 2000))
+            t_total = 0.0
+            for kk in (1, 10, 100):
+                for e in np.unique(ef[sample][k[sample] == kk]):
+                    rows = sample[(k[sample] == kk) & (ef[sample] == e)]
+                    idx.setQueryTimeParams({"efSearch": int(e)})
+                    t0 = time.perf_counter()
+                    idx.knnQueryBatch(queries[rows], k=int(kk), num_threads=os.cpu_count())
+                    t_total += time.perf_counter() - t0
+            out["cpu_reference"] = {"qps": round(len(sample) / t_total), "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": f"{len(sample)} queries of the mixed batch, grouped by (k, efSearch)"}
+    print(json.dumps(out))
+
+
+def reference_module_or_none():
+    from oracle.oracle import reference_module
+    return reference_module()
+
+
 # ------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -241,9 +410,15 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile-case", type=int, default=0, metavar="NQ",
                     help="profiling run: only NQ queries at the headline efSearch, no sweep, no baselines")
+    ap.add_argument("--workload", choices=["c2", "c3", "c4", "c5"], default="c2",
+                    help="c2 (default, the headline line); c3 cosine 1M x 100 + brute force; c4 negdot "
+                         "1M x 960 mixed k/ef batch; c5 l2 5M x 96 serving")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload != "c2":
+        run_aux(args)
+        return
 
     rank, world, local = dist_init(args.gpus)
     base, queries, space, m = workload_data()
@@ -284,11 +459,11 @@ def main():
     d_counts = torch.empty((nq,), dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream()
 
-    def run_device(plain=False):
+    def run_device(plain=False, graph=False):
+        flags = _capi.FLAG_DEVICE_PTRS | (_capi.FLAG_PLAIN_KERNEL if plain else 0) | (
+            _capi.FLAG_CUDA_GRAPH if graph else 0)
         rc = lib.nmsg_knn_batch(index._h, dq.data_ptr(), nq, dim, K, None, None, K, d_ids.data_ptr(),
-                                d_dists.data_ptr(), d_counts.data_ptr(), None,
-                                _capi.FLAG_DEVICE_PTRS | (_capi.FLAG_PLAIN_KERNEL if plain else 0),
-                                stream.cuda_stream)
+                                d_dists.data_ptr(), d_counts.data_ptr(), None, flags, stream.cuda_stream)
         _capi.check(rc)
 
     def time_device(steps, plain=False):
@@ -331,17 +506,21 @@ def main():
     _, _, _, st = index.knnQueryBatchArrays(queries, K, stats=True)
     alg_bytes = float(st[:, 3].sum())
     n_dist = float(st[:, 0].sum())
+    # launch shape picked by the autotuner on this batch (untimed); the timed steps use it
+    from nmslib_b200.autotune import autotune
+    best_shape, tune_table = autotune(index, queries, K, ef)
+    log(f"[bench] autotune: best {best_shape} " + " ".join(f"{s}:{ms:.3f}ms" for s, ms in tune_table))
 
-    # ---- timed: device-resident batches
+    # ---- timed: device-resident batches, each step one replay of the captured launch
     for _ in range(args.warmup):
-        run_device()
+        run_device(graph=True)
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
         for _ in range(args.steps):
-            run_device()
+            run_device(graph=True)
         end.record(stream)
         torch.cuda.synchronize()
     barrier(world)
@@ -365,6 +544,13 @@ def main():
     e2e_ms = e_start.elapsed_time(e_end) / e2e_steps
     e2e_ms = max_over_ranks(e2e_ms, world)
     e2e = world * nq / (e2e_ms * 1e-3)
+
+    # ---- serving: open-loop Poisson arrivals of the serving mix (batch 1..256 log-uniform,
+    # k in {10, 100}, efSearch in {100, 400}) against the same resident index
+    serving = serve_sweep(index, queries) if world == 1 else None
+
+    # ---- exact brute force on the tensor cores (same queries and vectors)
+    brute = brute_force_measure(index, queries) if world == 1 else None
 
     peak, peak_kind = peaks()
     achieved = alg_bytes / (ms * 1e-3) / 1e9
@@ -393,7 +579,12 @@ def main():
                              "distances_per_launch": n_dist},
                 "cpu_baseline": cpu,
                 "clocks": clk.summary(),
-                "sweep": sweep}
+                "sweep": sweep,
+                "launch": {"autotuned_shape": {"warps_per_block": best_shape[0], "rows_per_group": best_shape[1],
+                                               "visited_hash_log2": best_shape[2], "stage_rows": best_shape[3]},
+                           "cuda_graph": True},
+                "serving": serving,
+                "bruteforce": brute}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -417,6 +417,7 @@ namespace nmsg {
 
 struct BruteForceState {
   int kp = 0;       // padded dim (multiple of 64, <= 256)
+  float max_xn = 0; // largest |x|^2 over the base (l2 bound)
   DevBuf x16, x32, xn, xn_hi, xn_lo, xt_max, dx_max;
   DevBuf q32, q16, qn_hi, qn_lo, eps, cand_key, cand_id, tau, needs, qact, coll_id, coll_key, coll_cnt;
   DevBuf out_id, out_key, out_cnt, scr_id, scr_key, fin_id, fin_key, fin_cnt, status;
@@ -617,7 +618,15 @@ int prepare_base(nmsg_index* h, BruteForceState* s) {
   const int dim = hi.dim;
   s->kp = ((dim + BK - 1) / BK) * BK;
   std::vector<float> x((size_t)n * dim);
-  for (int64_t i = 0; i < n; ++i) std::memcpy(x.data() + i * dim, hi.vec(i), 4 * dim);
+  double max_xn = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const float* v = hi.vec(i);
+    std::memcpy(x.data() + i * dim, v, 4 * dim);
+    double a = 0;
+    for (int e = 0; e < dim; ++e) a += (double)v[e] * v[e];
+    max_xn = std::max(max_xn, a);
+  }
+  s->max_xn = (float)max_xn;
   BF_CUDA(s->x32.ensure(x.size() * 4, false), "cudaMalloc(brute-force fp32 base)");
   BF_CUDA(cudaMemcpy(s->x32.p, x.data(), x.size() * 4, cudaMemcpyHostToDevice), "upload base");
   BF_CUDA(s->x16.ensure((size_t)n * s->kp * 2, false), "cudaMalloc(bf16 base)");
@@ -708,16 +717,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   BF_CUDA(s->scr_id.ensure((size_t)nq * k * 4, false), "cudaMalloc");
   BF_CUDA(s->scr_key.ensure((size_t)nq * k * 8, false), "cudaMalloc");
   BF_CUDA(s->status.ensure(4, true), "cudaMalloc");
-  float max_xn = 0.0f;
-  if (l2) {
-    // largest |x|^2 for the l2 bound (computed once on the host from the index rows)
-    for (int64_t i = 0; i < n; ++i) {
-      const float* v = hi.vec(i);
-      double a = 0;
-      for (int e = 0; e < dim; ++e) a += (double)v[e] * v[e];
-      max_xn = std::max(max_xn, (float)a);
-    }
-  }
+  const float max_xn = s->max_xn;
   prep_query_kernel<<<(mpad + 7) / 8, 256, 0, st>>>(qin, (int)nq, dim, kp, mpad, cosine, l2, s->xt_max.as<unsigned>(),
                                                      s->dx_max.as<unsigned>(), max_xn * 1.0001f, s->q32.as<float>(),
                                                      s->q16.as<__nv_bfloat16>(), s->qn_hi.as<float>(),

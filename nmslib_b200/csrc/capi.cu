@@ -217,6 +217,7 @@ void nmsg_index_free(nmsg_index* h) {
   {
     DeviceGuard g(h->device);
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
     destroy_bruteforce(h->bf);
     h->bf = nullptr;
     for (DevBuf* b : {&h->vecs, &h->l0, &h->up_off, &h->up_links, &h->ext_id, &h->visited, &h->epochs, &h->locks,
@@ -420,12 +421,16 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
     if (!same) {
       if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
       h->graph_exec = nullptr;
-      NMSG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
-      cudaMemsetAsync(a.work_counter, 0, 4, st);
-      cudaMemsetAsync(a.status, 0, 4, st);
-      const int lrc = launch_search(a, plain, gather, any_old, blocks, wpb, stream);
+      // capture on the handle's own stream (the legacy default stream cannot be captured); the
+      // graph is then launched on the caller's stream
+      if (!h->capture_stream) NMSG_CUDA(cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking), "stream");
+      cudaStream_t cs = h->capture_stream;
+      NMSG_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+      cudaMemsetAsync(a.work_counter, 0, 4, cs);
+      cudaMemsetAsync(a.status, 0, 4, cs);
+      const int lrc = launch_search(a, plain, gather, any_old, blocks, wpb, cs);
       cudaGraph_t graph = nullptr;
-      const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+      const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
       if (lrc != 0 || ce != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         return cuda_fail(ce != cudaSuccess ? ce : (cudaError_t)lrc, "capture search launch");

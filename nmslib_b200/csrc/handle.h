@@ -99,6 +99,7 @@ struct nmsg_index {
   nmsg_launch_config cfg{0, 0, 0, 0};
   nmsg::BruteForceState* bf = nullptr;  // brute-force data, built on first use
   cudaGraphExec_t graph_exec = nullptr;  // last captured device-pointer search (NMSG_CUDA_GRAPH)
+  cudaStream_t capture_stream = nullptr;
   nmsg::SearchArgs graph_args{};
   int graph_shape[5] = {0, 0, 0, 0, 0};
   std::mutex mu;

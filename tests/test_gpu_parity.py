@@ -154,3 +154,30 @@ def test_launch_shapes_do_not_change_results(name, si, cfg):
             np.testing.assert_array_equal(st, ost)
     finally:
         idx.setLaunchConfig(0, 0, 0)
+
+
+def test_cuda_graph_launch_matches():
+    """NMSG_CUDA_GRAPH: the captured launch replays with identical results, and a change of
+    arguments (efSearch) re-captures."""
+    import torch
+
+    from nmslib_b200 import _capi
+    idx = _gpu_index("c1_l2_d128")
+    lib = _capi.load()
+    q = np.ascontiguousarray(load_golden("c1_l2_d128")["queries"])
+    nq, dim = q.shape
+    dq = torch.from_numpy(q).cuda()
+    for ef in (100, 40, 100):
+        idx.setQueryTimeParams({"efSearch": ef})
+        want = idx.knnQueryBatchArrays(q, 10)
+        for _ in range(3):
+            ids = torch.full((nq, 10), -7, dtype=torch.int32, device="cuda")
+            d = torch.zeros((nq, 10), dtype=torch.float32, device="cuda")
+            c = torch.zeros((nq,), dtype=torch.int32, device="cuda")
+            rc = lib.nmsg_knn_batch(idx._h, dq.data_ptr(), nq, dim, 10, None, None, 10, ids.data_ptr(),
+                                    d.data_ptr(), c.data_ptr(), None,
+                                    _capi.FLAG_DEVICE_PTRS | _capi.FLAG_CUDA_GRAPH, None)
+            assert rc == 0, _capi.last_error()
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(ids.cpu().numpy(), want[0])
+            np.testing.assert_array_equal(c.cpu().numpy(), want[2])
