@@ -71,13 +71,21 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """Max of a per-rank scalar over all ranks (NCCL tensors on the GPU, gloo on the CPU)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_throughput(nq_per_rank, ms_per_rank, world):
+    """Whole-job queries/s of `world` replicas that each searched nq_per_rank queries: the job
+    takes as long as its slowest rank."""
+    return world * nq_per_rank / (max_over_ranks(ms_per_rank, world) * 1e-3)
 
 
 # ------------------------------------------------------------------ data and index
@@ -526,7 +534,7 @@ def main():
     barrier(world)
     ms = start.elapsed_time(end) / args.steps
     ms_max = max_over_ranks(ms, world)
-    value = world * nq / (ms_max * 1e-3)
+    value = world * nq / (ms_max * 1e-3)  # == replica_throughput(nq, ms, world)
 
     # ---- timed: end to end through the public API with host arrays
     h_q = np.ascontiguousarray(queries)

@@ -41,25 +41,28 @@ using namespace sm100;
 constexpr int BM = 128;                 // queries per tile = TMEM lanes
 constexpr int BN = 256;                 // base rows per tile = accumulator columns
 constexpr int BK = 64;                  // bf16 elements per 128-byte swizzle row
-constexpr int STAGES = 3;               // base-tile pipeline depth
-constexpr int CAND = 32;                // candidates kept per query per chunk (pass A)
+constexpr int CAND = 32;                // candidates kept per query per list (pass A)
 constexpr int KB_MAX = 4;               // padded dim <= 256
 constexpr int Q_BLOCK_BYTES = BM * BK * 2;   // 16 KB
 constexpr int X_STAGE_BYTES = BN * BK * 2;   // 32 KB
-constexpr int kThreads = 192;           // warps 0-3 epilogue, 4 TMA, 5 MMA
+constexpr int EPI_WARPS = 8;            // two warps per TMEM lane quarter, one per column half
+constexpr int HALVES = 2;
+constexpr int kThreads = (EPI_WARPS + 2) * 32;  // + TMA warp + MMA warp
+constexpr int LIST_STRIDE = CAND + 1;   // +1: rows of a list on different banks
 
 struct GemmArgs {
   int kb;             // padded dim / 64
+  int stages;         // base-tile pipeline depth (3 when kb <= 2, else 2)
   int n;              // base rows
   int nq;             // queries
   int n_tiles;        // ceil(n / BN)
   int chunk_tiles;    // base tiles per work item
   int n_chunks;
   int q_blocks;
-  int mode;           // 0: top-CAND per chunk; 1: collect keys >= tau
+  int mode;           // 0: top-CAND per (chunk, column half); 1: collect keys >= tau
   int key_l2;         // 1: key = 2 dot - |x|^2
-  const float* xnorm2;
-  float* cand_key;    // [nq][n_chunks][CAND]
+  const float* xnorm2;  // padded to n_tiles * BN
+  float* cand_key;    // [nq][n_chunks * HALVES][CAND]
   int32_t* cand_id;
   const float* tau;   // [nq]
   const uint8_t* q_active;  // [q_blocks * BM]
@@ -70,15 +73,17 @@ struct GemmArgs {
   int32_t* status;
 };
 
-struct __align__(1024) GemmSmem {
-  uint8_t q[KB_MAX][Q_BLOCK_BYTES];
-  uint8_t x[STAGES][X_STAGE_BYTES];
-  float ckey[BM][CAND + 1];  // +1: rows on different banks
-  int32_t cid[BM][CAND + 1];
-  uint64_t x_full[STAGES], x_empty[STAGES];
-  uint64_t q_full, q_empty;
-  uint64_t acc_full[2], acc_empty[2];
-  uint32_t tmem_base;
+// Shared memory: Q blocks | base stages | candidate lists | barriers (1024-aligned base).
+struct SmemLayout {
+  int q_off, x_off, key_off, id_off, bar_off, total;
+  __host__ __device__ SmemLayout(int kb, int stages) {
+    q_off = 0;
+    x_off = q_off + kb * Q_BLOCK_BYTES;
+    key_off = x_off + stages * X_STAGE_BYTES;
+    id_off = key_off + HALVES * BM * LIST_STRIDE * 4;
+    bar_off = (id_off + HALVES * BM * LIST_STRIDE * 4 + 7) & ~7;
+    total = bar_off + 8 * (2 * 4 + 2 + 4) + 16;
+  }
 };
 
 __device__ __forceinline__ bool item_active(const GemmArgs& a, int qb) {
@@ -89,33 +94,83 @@ __device__ __forceinline__ bool item_active(const GemmArgs& a, int qb) {
   return false;
 }
 
+// A row's candidate list is a min-heap of CAND (key, column) pairs in shared memory: the root is
+// the smallest kept key, i.e. the threshold a new key must beat. The first CAND offers fill it,
+// then it is heapified once; later insertions replace the root and sift down (log2 CAND steps).
+__device__ __forceinline__ void heap_sift_down(float* lk, int32_t* li, int pos) {
+  const float key = lk[pos];
+  const int32_t id = li[pos];
+  while (true) {
+    int child = 2 * pos + 1;
+    if (child >= CAND) break;
+    if (child + 1 < CAND && lk[child + 1] < lk[child]) ++child;
+    if (!(lk[child] < key)) break;
+    lk[pos] = lk[child];
+    li[pos] = li[child];
+    pos = child;
+  }
+  lk[pos] = key;
+  li[pos] = id;
+}
+
+__device__ __forceinline__ void list_offer(float* lk, int32_t* li, int& nfill, float& thr, float key, int col) {
+  if (nfill < CAND) {
+    lk[nfill] = key;
+    li[nfill] = col;
+    if (++nfill == CAND) {
+      for (int p = CAND / 2 - 1; p >= 0; --p) heap_sift_down(lk, li, p);
+      thr = lk[0];
+    }
+    return;
+  }
+  if (!(key > thr)) return;
+  lk[0] = key;
+  li[0] = col;
+  heap_sift_down(lk, li, 0);
+  thr = lk[0];
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     bf16_scan_kernel(const __grid_constant__ CUtensorMap tmq, const __grid_constant__ CUtensorMap tmx, GemmArgs a) {
   extern __shared__ uint8_t smem_raw[];
-  GemmSmem& s = *reinterpret_cast<GemmSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const SmemLayout L(a.kb, a.stages);
+  uint8_t* sq = base + L.q_off;
+  uint8_t* sx = base + L.x_off;
+  float* skey = reinterpret_cast<float*>(base + L.key_off);
+  int32_t* sid = reinterpret_cast<int32_t*>(base + L.id_off);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + L.bar_off);
+  uint64_t* x_full = bars;          // [4]
+  uint64_t* x_empty = bars + 4;     // [4]
+  uint64_t* q_full = bars + 8;
+  uint64_t* q_empty = bars + 9;
+  uint64_t* acc_full = bars + 10;   // [2]
+  uint64_t* acc_empty = bars + 12;  // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 14);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n_items = a.q_blocks * a.n_chunks;
+  const int stages = a.stages;
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < STAGES; ++i) {
-      mbar_init(&s.x_full[i], 1);
-      mbar_init(&s.x_empty[i], 1);
+    for (int i = 0; i < stages; ++i) {
+      mbar_init(&x_full[i], 1);
+      mbar_init(&x_empty[i], 1);
     }
-    mbar_init(&s.q_full, 1);
-    mbar_init(&s.q_empty, 1);
+    mbar_init(q_full, 1);
+    mbar_init(q_empty, 1);
     for (int i = 0; i < 2; ++i) {
-      mbar_init(&s.acc_full[i], 1);
-      mbar_init(&s.acc_empty[i], 4);  // one arrival per epilogue warp
+      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_empty[i], EPI_WARPS);  // one arrival per epilogue warp
     }
     fence_barrier_init();
   }
-  if (warp == 0) tmem_alloc(&s.tmem_base, 512);
+  if (warp == 0) tmem_alloc(tmem_slot, 512);
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = s.tmem_base;
+  const uint32_t tmem = *tmem_slot;
   bool ok = true;
 
-  if (warp == 4) {
+  if (warp == EPI_WARPS) {
     // ------------------------------------------------ TMA producer
     if (lane == 0) {
       prefetch_tmap(&tmq);
@@ -127,18 +182,18 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int qb = item / a.n_chunks, chunk = item % a.n_chunks;
         if (!item_active(a, qb)) continue;
         if (done_items > 0) {
-          ok = mbar_wait(&s.q_empty, qphase);
+          ok = mbar_wait(q_empty, qphase);
           qphase ^= 1;
         }
-        mbar_arrive_expect_tx(&s.q_full, a.kb * Q_BLOCK_BYTES);
-        for (int kb = 0; kb < a.kb; ++kb) tma_load_2d(s.q[kb], &tmq, &s.q_full, kb * BK, qb * BM);
+        mbar_arrive_expect_tx(q_full, a.kb * Q_BLOCK_BYTES);
+        for (int kb = 0; kb < a.kb; ++kb) tma_load_2d(sq + kb * Q_BLOCK_BYTES, &tmq, q_full, kb * BK, qb * BM);
         const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
         for (int t = t0; t < t1 && ok; ++t) {
           for (int kb = 0; kb < a.kb && ok; ++kb) {
-            ok = mbar_wait(&s.x_empty[stage], xphase ^ 1);
-            mbar_arrive_expect_tx(&s.x_full[stage], X_STAGE_BYTES);
-            tma_load_2d(s.x[stage], &tmx, &s.x_full[stage], kb * BK, t * BN);
-            if (++stage == STAGES) {
+            ok = mbar_wait(&x_empty[stage], xphase ^ 1);
+            mbar_arrive_expect_tx(&x_full[stage], X_STAGE_BYTES);
+            tma_load_2d(sx + stage * X_STAGE_BYTES, &tmx, &x_full[stage], kb * BK, t * BN);
+            if (++stage == stages) {
               stage = 0;
               xphase ^= 1;
             }
@@ -147,7 +202,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         ++done_items;
       }
     }
-  } else if (warp == 5) {
+  } else if (warp == EPI_WARPS + 1) {
     // ------------------------------------------------ MMA issuer
     if (lane == 0) {
       const uint32_t idesc = idesc_bf16_f32(BM, BN);
@@ -158,37 +213,41 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
         const int qb = item / a.n_chunks, chunk = item % a.n_chunks;
         if (!item_active(a, qb)) continue;
-        ok = mbar_wait(&s.q_full, qphase);
+        ok = mbar_wait(q_full, qphase);
         qphase ^= 1;
         tc_fence_after();
         const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
         for (int t = t0; t < t1 && ok; ++t, ++tcount) {
           const int buf = tcount & 1;
-          ok = mbar_wait(&s.acc_empty[buf], accphase[buf] ^ 1);
+          ok = mbar_wait(&acc_empty[buf], accphase[buf] ^ 1);
           accphase[buf] ^= 1;
           tc_fence_after();
           const uint32_t dcol = tmem + buf * BN;
           for (int kb = 0; kb < a.kb && ok; ++kb) {
-            ok = mbar_wait(&s.x_full[stage], xphase);
+            ok = mbar_wait(&x_full[stage], xphase);
             tc_fence_after();
-            const uint32_t qa = smem_u32(s.q[kb]), xa = smem_u32(s.x[stage]);
+            const uint32_t qa = smem_u32(sq + kb * Q_BLOCK_BYTES), xa = smem_u32(sx + stage * X_STAGE_BYTES);
 #pragma unroll
             for (int k = 0; k < BK / 16; ++k)
               umma_bf16(dcol, smem_desc_sw128(qa + 32 * k), smem_desc_sw128(xa + 32 * k), idesc, kb > 0 || k > 0);
-            umma_commit(&s.x_empty[stage]);
-            if (++stage == STAGES) {
+            umma_commit(&x_empty[stage]);
+            if (++stage == stages) {
               stage = 0;
               xphase ^= 1;
             }
           }
-          umma_commit(&s.acc_full[buf]);
+          umma_commit(&acc_full[buf]);
         }
-        umma_commit(&s.q_empty);
+        umma_commit(q_empty);
       }
     }
   } else {
-    // ------------------------------------------------ epilogue: warps 0-3, thread = query row
-    const int row = warp * 32 + lane;
+    // ------------------------------------------------ epilogue: warps 0-7; thread = one query row
+    // (TMEM lane) for one half of the tile's columns
+    const int quarter = warp & 3, half = warp >> 2;
+    const int row = quarter * 32 + lane;
+    float* lk = skey + (half * BM + row) * LIST_STRIDE;
+    int32_t* li = sid + (half * BM + row) * LIST_STRIDE;
     uint32_t accphase[2] = {0, 0};
     int tcount = 0;
     for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
@@ -196,68 +255,77 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!item_active(a, qb)) continue;
       const int q = qb * BM + row;
       const bool qvalid = q < a.nq;
-      float thr = -INFINITY;  // mode 0: current C-th best; mode 1: tau
-      int nfill = 0, minpos = 0;
+      float thr = -INFINITY;  // mode 0: the list's smallest key once full; mode 1: tau
+      int nfill = 0;
       if (a.mode == 1) thr = (qvalid && a.q_active[q]) ? a.tau[q] : INFINITY;
       const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
+      // |x|^2 of this half's 128 columns, 4 per lane, loaded one tile ahead and handed to the
+      // other lanes by shuffles
+      const float4* xn4 = reinterpret_cast<const float4*>(a.xnorm2) + half * (BN / HALVES / 4) + lane;
+      float4 nrm_next = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (a.key_l2 && t0 < t1) nrm_next = __ldg(xn4 + (size_t)t0 * (BN / 4));
       for (int t = t0; t < t1 && ok; ++t, ++tcount) {
         const int buf = tcount & 1;
-        ok = mbar_wait(&s.acc_full[buf], accphase[buf]);
+        const float4 nrm = nrm_next;
+        if (a.key_l2 && t + 1 < t1) nrm_next = __ldg(xn4 + (size_t)(t + 1) * (BN / 4));
+        ok = mbar_wait(&acc_full[buf], accphase[buf]);
         accphase[buf] ^= 1;
         tc_fence_after();
-        for (int c = 0; c < BN / 32; ++c) {
+#pragma unroll 1
+        for (int c = 0; c < BN / 32 / HALVES; ++c) {
+          const int ccol = half * (BN / HALVES) + c * 32;  // column inside the tile
           float v[32];
-          tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + buf * BN + c * 32, v);
-          const int col0 = t * BN + c * 32;
+          tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + buf * BN + ccol, v);
+          const int col0 = t * BN + ccol;
+          // keys of all 32 columns without branches (independent, so they overlap), then one
+          // test of their maximum against the threshold; the per-column path runs only if it passes
+          if (a.key_l2) {
 #pragma unroll
-          for (int i = 0; i < 32; ++i) {
-            const int col = col0 + i;
-            if (col >= a.n) continue;
-            float key = v[i];
-            if (a.key_l2) key = __fsub_rn(__fmul_rn(2.0f, key), __ldg(a.xnorm2 + col));
-            if (a.mode == 0) {
-              if (nfill < CAND) {
-                s.ckey[row][nfill] = key;
-                s.cid[row][nfill] = col;
-                if (++nfill == CAND) {
-                  thr = s.ckey[row][0];
-                  minpos = 0;
-                  for (int j = 1; j < CAND; ++j)
-                    if (s.ckey[row][j] < thr) {
-                      thr = s.ckey[row][j];
-                      minpos = j;
-                    }
-                }
-              } else if (key > thr) {
-                s.ckey[row][minpos] = key;
-                s.cid[row][minpos] = col;
-                thr = s.ckey[row][0];
-                minpos = 0;
-                for (int j = 1; j < CAND; ++j)
-                  if (s.ckey[row][j] < thr) {
-                    thr = s.ckey[row][j];
-                    minpos = j;
-                  }
-              }
-            } else if (key >= thr) {
-              const int slot = atomicAdd(a.coll_cnt + q, 1);
-              if (slot < a.coll_cap) {
-                a.coll_id[(size_t)q * a.coll_cap + slot] = col;
-                a.coll_key[(size_t)q * a.coll_cap + slot] = key;
-              }
+            for (int i = 0; i < 32; ++i) {
+              const float comp = (i & 3) == 0 ? nrm.x : (i & 3) == 1 ? nrm.y : (i & 3) == 2 ? nrm.z : nrm.w;
+              const float xn = __shfl_sync(0xffffffffu, comp, c * 8 + (i >> 2));
+              v[i] = __fsub_rn(__fmul_rn(2.0f, v[i]), xn);
             }
+          }
+          if (col0 + 32 > a.n) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+              if (col0 + i >= a.n) v[i] = -INFINITY;
+          }
+          float mx = v[0];
+#pragma unroll
+          for (int i = 1; i < 32; ++i) mx = fmaxf(mx, v[i]);
+          if (a.mode == 0) {
+            if (mx > thr || nfill < CAND) {
+#pragma unroll
+              for (int i = 0; i < 32; ++i)
+                if (v[i] > thr || nfill < CAND) {
+                  if (col0 + i < a.n) list_offer(lk, li, nfill, thr, v[i], col0 + i);
+                }
+            }
+          } else if (mx >= thr) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+              if (v[i] >= thr) {
+                const int slot = atomicAdd(a.coll_cnt + q, 1);
+                if (slot < a.coll_cap) {
+                  a.coll_id[(size_t)q * a.coll_cap + slot] = col0 + i;
+                  a.coll_key[(size_t)q * a.coll_cap + slot] = v[i];
+                }
+              }
           }
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&s.acc_empty[buf]);
+        if (lane == 0) mbar_arrive(&acc_empty[buf]);
       }
       if (a.mode == 0 && qvalid) {
-        float* ok_out = a.cand_key + ((size_t)q * a.n_chunks + chunk) * CAND;
-        int32_t* oi_out = a.cand_id + ((size_t)q * a.n_chunks + chunk) * CAND;
+        const size_t list = (size_t)q * a.n_chunks * HALVES + chunk * HALVES + half;
+        float* ok_out = a.cand_key + list * CAND;
+        int32_t* oi_out = a.cand_id + list * CAND;
         for (int j = 0; j < CAND; ++j) {
-          ok_out[j] = j < nfill ? s.ckey[row][j] : -INFINITY;
-          oi_out[j] = j < nfill ? s.cid[row][j] : -1;
+          ok_out[j] = j < nfill ? lk[j] : -INFINITY;
+          oi_out[j] = j < nfill ? li[j] : -1;
         }
       }
     }
@@ -315,90 +383,181 @@ struct RerankArgs {
   const float* xn_hi;    // l2: |x|^2 as double-float
   const float* xn_lo;
   int dim, n, nq, k, l2;
-  int n_lists, list_len;       // candidate lists per query and their length
-  const int32_t* ids;          // [nq][n_lists * list_len] (-1 = empty)
-  const float* bf_keys;        // same shape, BF16 keys (pass A only, for the certificate)
+  int n_lists, list_len;       // pass A: candidate lists per query and their length
+  const int32_t* ids;          // pass A: [nq][n_lists * list_len] (-1 = empty); pass B: [nq][coll_cap]
+  const float* bf_keys;        // BF16 keys, same layout
   const int32_t* list_count;   // pass B: per-query count (null in pass A)
   const float* eps;            // [nq] bound on |BF16 key - exact key|
+  int coll_cap;
   // outputs
-  int32_t* out_ids;            // [nq][k]
+  int32_t* out_ids;            // [nq][k] internal ids, best first
   DF* out_keys;                // [nq][k]
   int32_t* out_count;          // [nq]
-  float* tau;                  // [nq] collection threshold (pass A), else unused
-  uint8_t* needs;              // [nq] 1 = not certified (pass A) / overflowed (pass B)
-  int coll_cap;
-  int32_t* scratch_id;         // [nq][k] working top-k ids per warp slot
-  DF* scratch_key;
+  float* tau;                  // pass A: [nq] threshold for the second pass
+  uint8_t* needs;              // pass A: 1 = not certified; pass B: 1 = collection overflowed
 };
 
-// One warp per query: exact keys for every listed candidate, top-k by (key desc, id asc).
+// (key, id) order of the result: larger key first, then smaller id.
+__device__ __forceinline__ bool better(DF ka, int ia, DF kb, int ib) {
+  return df_greater(ka, kb) || (ka.hi == kb.hi && ka.lo == kb.lo && ia < ib);
+}
+
+// Exact key of one (query, row) pair computed by a single lane (sequential over the dimension).
+__device__ DF exact_key_lane(const float* __restrict__ q, const float* __restrict__ x, int dim, bool l2, DF xnorm) {
+  DF acc{0.0f, 0.0f};
+  for (int e = 0; e < dim; ++e) acc = df_add_df(acc, df_mul_ff(q[e], __ldg(x + e)));
+  if (l2) return df_add_df(DF{__fmul_rn(2.0f, acc.hi), __fmul_rn(2.0f, acc.lo)}, DF{-xnorm.hi, -xnorm.lo});
+  return acc;
+}
+
+// One warp per query:
+//  1. B_k = the k-th largest BF16 key among the candidates (pairs (key, slot), k rounds of
+//     warp max);
+//  2. only candidates with BF16 key >= B_k - 2 eps can be in the exact top k (the k candidates
+//     at or above B_k all have exact keys >= B_k - eps, anything below B_k - 2 eps has an exact
+//     key < B_k - eps), so only they get exact keys, one candidate per lane;
+//  3. the exact top k by (key desc, id asc), merged 32 candidates at a time;
+//  4. pass A: the certificate and the second-pass threshold.
 __global__ void rerank_kernel(RerankArgs a) {
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (q >= a.nq) return;
-  const float* qv = a.q + (size_t)q * a.dim;
-  int32_t* tid = a.scratch_id + (size_t)q * a.k;
-  DF* tkey = a.scratch_key + (size_t)q * a.k;
-  int have = 0;
-  int total = a.n_lists * a.list_len;
-  if (a.list_count) total = min(a.list_count[q], a.coll_cap);
-  float worst_bf_chunk = -INFINITY;  // max over chunks of each chunk's C-th best BF16 key
-  if (!a.list_count) {
+  const bool pass_b = a.list_count != nullptr;
+  int total = pass_b ? min(a.list_count[q], a.coll_cap) : a.n_lists * a.list_len;
+  const size_t base = pass_b ? (size_t)q * a.coll_cap : (size_t)q * a.n_lists * a.list_len;
+  const int32_t* ids = a.ids + base;
+  const float* bk = a.bf_keys + base;
+  const float eps = a.eps[q];
+
+  // pass A: every full list bounds the vectors it dropped by its smallest key
+  float worst_bf_list = -INFINITY;
+  if (!pass_b) {
     for (int c = 0; c < a.n_lists; ++c) {
-      // a full chunk list bounds every vector of the chunk it dropped by its smallest key
       float mn = INFINITY;
       bool full = true;
       for (int j = lane; j < a.list_len; j += 32) {
-        const int id = a.ids[(size_t)q * total + c * a.list_len + j];
-        full &= id >= 0;
-        mn = fminf(mn, a.bf_keys[(size_t)q * total + c * a.list_len + j]);
+        full &= ids[c * a.list_len + j] >= 0;
+        mn = fminf(mn, bk[c * a.list_len + j]);
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-      full = __all_sync(0xffffffffu, full);
-      if (full) worst_bf_chunk = fmaxf(worst_bf_chunk, mn);
+      if (__all_sync(0xffffffffu, full)) worst_bf_list = fmaxf(worst_bf_list, mn);
     }
   }
-  for (int t = 0; t < total; ++t) {
-    const int id = a.list_count ? a.ids[(size_t)q * a.coll_cap + t] : a.ids[(size_t)q * total + t];
-    if (id < 0) continue;
-    DF xn{0.0f, 0.0f};
-    if (a.l2) xn = DF{a.xn_hi[id], a.xn_lo[id]};
-    const DF key = exact_key(qv, a.x + (size_t)id * a.dim, a.dim, a.l2, xn);
-    // insert into the running top-k (sorted: best first); lane 0 does it
-    if (lane == 0) {
-      int pos = have;
-      while (pos > 0) {
-        const DF pk = tkey[pos - 1];
-        const int pid = tid[pos - 1];
-        if (df_greater(pk, key) || (pk.hi == key.hi && pk.lo == key.lo && pid < id)) break;
-        if (pos < a.k) {
-          tkey[pos] = pk;
-          tid[pos] = pid;
+
+  // 1. k-th largest BF16 key (pairs ordered by key desc, slot asc)
+  float prev_k = INFINITY;
+  int prev_s = -1;
+  int found = 0;
+  for (int r = 0; r < a.k; ++r) {
+    float bkey = -INFINITY;
+    int bslot = 0x7fffffff;
+    for (int t = lane; t < total; t += 32) {
+      if (ids[t] < 0) continue;
+      const float kv = bk[t];
+      const bool below = kv < prev_k || (kv == prev_k && t > prev_s);  // after the previous pick
+      if (below && (kv > bkey || (kv == bkey && t < bslot))) {
+        bkey = kv;
+        bslot = t;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ok = __shfl_xor_sync(0xffffffffu, bkey, o);
+      const int os = __shfl_xor_sync(0xffffffffu, bslot, o);
+      if (ok > bkey || (ok == bkey && os < bslot)) {
+        bkey = ok;
+        bslot = os;
+      }
+    }
+    if (bslot == 0x7fffffff) break;
+    prev_k = bkey;
+    prev_s = bslot;
+    ++found;
+  }
+  const float cut = found == a.k ? __fsub_rd(prev_k, __fmul_ru(2.0f, eps)) : -INFINITY;
+
+  // 2-3. exact keys of the candidates at or above the cut, one per lane, merged into the top k
+  const float* qv = a.q + (size_t)q * a.dim;
+  DF top_k = DF{-INFINITY, 0.0f};  // lane j holds the j-th best so far (j < k)
+  int top_i = 0x7fffffff;
+  int have = 0;
+  for (int t0 = 0; t0 < total; t0 += 32) {
+    const int t = t0 + lane;
+    int id = -1;
+    if (t < total) {
+      id = ids[t];
+      if (id >= 0 && !(bk[t] >= cut)) id = -1;
+    }
+    if (__ballot_sync(0xffffffffu, id >= 0) == 0) continue;
+    DF key{-INFINITY, 0.0f};
+    if (id >= 0) {
+      DF xn{0.0f, 0.0f};
+      if (a.l2) xn = DF{a.xn_hi[id], a.xn_lo[id]};
+      key = exact_key_lane(qv, a.x + (size_t)id * a.dim, a.dim, a.l2, xn);
+    }
+    // merge: the new top k = the k best of (old top k held by lanes < have) and the 32 new ones
+    DF nk{-INFINITY, 0.0f};
+    int ni = 0x7fffffff;
+    bool my_old = lane < have, my_new = id >= 0;
+    int taken = 0;
+    for (int r = 0; r < a.k; ++r) {
+      // candidate of this lane: its better remaining entry
+      DF ck{-INFINITY, 0.0f};
+      int ci = 0x7fffffff, cw = -1;  // which: 0 old, 1 new
+      if (my_old && (!my_new || better(top_k, top_i, key, id))) {
+        ck = top_k;
+        ci = top_i;
+        cw = 0;
+      } else if (my_new) {
+        ck = key;
+        ci = id;
+        cw = 1;
+      }
+      DF bkk = ck;
+      int bi = ci, bl = cw >= 0 ? lane : 32;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const DF ok{__shfl_xor_sync(0xffffffffu, bkk.hi, o), __shfl_xor_sync(0xffffffffu, bkk.lo, o)};
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        const int ol = __shfl_xor_sync(0xffffffffu, bl, o);
+        if (ol < 32 && (bl == 32 || better(ok, oi, bkk, bi))) {
+          bkk = ok;
+          bi = oi;
+          bl = ol;
         }
-        --pos;
       }
-      if (pos < a.k) {
-        tkey[pos] = key;
-        tid[pos] = id;
+      if (bl == 32) break;
+      if (lane == bl) {
+        if (cw == 0)
+          my_old = false;
+        else
+          my_new = false;
       }
+      if (lane == r) {
+        nk = bkk;
+        ni = bi;
+      }
+      ++taken;
     }
-    have = min(have + 1, a.k);
-    __syncwarp();
+    top_k = nk;
+    top_i = ni;
+    have = taken;
   }
+  // 4. outputs
+  const int kk = a.k;
+  if (lane < kk) {
+    a.out_ids[(size_t)q * kk + lane] = lane < have ? top_i : -1;
+    a.out_keys[(size_t)q * kk + lane] = lane < have ? top_k : DF{-INFINITY, 0.0f};
+  }
+  const float kth = __shfl_sync(0xffffffffu, top_k.hi, kk - 1);
   if (lane == 0) {
-    for (int j = 0; j < a.k; ++j) {
-      a.out_ids[(size_t)q * a.k + j] = j < have ? tid[j] : -1;
-      a.out_keys[(size_t)q * a.k + j] = j < have ? tkey[j] : DF{-INFINITY, 0.0f};
-    }
     a.out_count[q] = have;
-    if (!a.list_count) {
-      // certificate: every vector outside the candidates has BF16 key <= worst_bf_chunk, so
-      // exact key <= worst_bf_chunk + eps; certified when that is below the k-th exact key
-      // tau <= exact k-th key - eps: the hi part alone can exceed the exact value by half an ulp
-      const float kth = have == a.k ? tkey[a.k - 1].hi : -INFINITY;
-      const float tau = __fsub_rd(__fsub_rd(kth, a.eps[q]), fabsf(kth) * 1.1920929e-7f);
-      const bool cert = have == a.n || (have == a.k && worst_bf_chunk < tau);
+    if (!pass_b) {
+      // every vector outside the lists has BF16 key <= worst_bf_list, so exact key <=
+      // worst_bf_list + eps; certified when that is below the k-th exact key (less half an ulp)
+      const float tau = have == kk ? __fsub_rd(__fsub_rd(kth, eps), fabsf(kth) * 1.1920929e-7f) : -INFINITY;
+      const bool cert = have == a.n || (have == kk && worst_bf_list < tau);
       a.tau[q] = tau;
       a.needs[q] = cert ? 0 : 1;
     } else {
@@ -630,7 +789,8 @@ int prepare_base(nmsg_index* h, BruteForceState* s) {
   BF_CUDA(s->x32.ensure(x.size() * 4, false), "cudaMalloc(brute-force fp32 base)");
   BF_CUDA(cudaMemcpy(s->x32.p, x.data(), x.size() * 4, cudaMemcpyHostToDevice), "upload base");
   BF_CUDA(s->x16.ensure((size_t)n * s->kp * 2, false), "cudaMalloc(bf16 base)");
-  BF_CUDA(s->xn.ensure(n * 4, false), "cudaMalloc(norms)");
+  const int64_t npad = ((n + BN - 1) / BN) * BN;  // the scan reads norms 32 at a time per tile
+  BF_CUDA(s->xn.ensure(npad * 4, true), "cudaMalloc(norms)");
   BF_CUDA(s->xn_hi.ensure(n * 4, false), "cudaMalloc(norms)");
   BF_CUDA(s->xn_lo.ensure(n * 4, false), "cudaMalloc(norms)");
   BF_CUDA(s->xt_max.ensure(dim * 4, true), "cudaMalloc(bounds)");
@@ -707,15 +867,13 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   BF_CUDA(s->qn_hi.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->qn_lo.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->eps.ensure(nq * 4, false), "cudaMalloc");
-  BF_CUDA(s->cand_key.ensure((size_t)nq * n_chunks * CAND * 4, false), "cudaMalloc");
-  BF_CUDA(s->cand_id.ensure((size_t)nq * n_chunks * CAND * 4, false), "cudaMalloc");
+  BF_CUDA(s->cand_key.ensure((size_t)nq * n_chunks * HALVES * CAND * 4, false), "cudaMalloc");
+  BF_CUDA(s->cand_id.ensure((size_t)nq * n_chunks * HALVES * CAND * 4, false), "cudaMalloc");
   BF_CUDA(s->tau.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->needs.ensure(mpad, false), "cudaMalloc");
   BF_CUDA(s->out_id.ensure((size_t)nq * k * 4, false), "cudaMalloc");
   BF_CUDA(s->out_key.ensure((size_t)nq * k * 8, false), "cudaMalloc");
   BF_CUDA(s->out_cnt.ensure(nq * 4, false), "cudaMalloc");
-  BF_CUDA(s->scr_id.ensure((size_t)nq * k * 4, false), "cudaMalloc");
-  BF_CUDA(s->scr_key.ensure((size_t)nq * k * 8, false), "cudaMalloc");
   BF_CUDA(s->status.ensure(4, true), "cudaMalloc");
   const float max_xn = s->max_xn;
   prep_query_kernel<<<(mpad + 7) / 8, 256, 0, st>>>(qin, (int)nq, dim, kp, mpad, cosine, l2, s->xt_max.as<unsigned>(),
@@ -735,6 +893,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ga.chunk_tiles = chunk_tiles;
   ga.n_chunks = n_chunks;
   ga.q_blocks = q_blocks;
+  ga.stages = kb <= 2 ? 3 : 2;
   ga.mode = 0;
   ga.key_l2 = l2;
   ga.xnorm2 = s->xn.as<float>();
@@ -743,7 +902,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ga.tau = s->tau.as<float>();
   ga.q_active = s->needs.as<uint8_t>();
   ga.status = s->status.as<int32_t>();
-  const int smem = (int)sizeof(GemmSmem) + 1024;
+  const int smem = SmemLayout(kb, ga.stages).total + 1024;
   BF_CUDA(cudaFuncSetAttribute(bf16_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
   const int grid = std::min(n_items, h->num_sms);
   bf16_scan_kernel<<<grid, kThreads, smem, st>>>(tmq, s->tmx, ga);
@@ -759,7 +918,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ra.nq = (int)nq;
   ra.k = k;
   ra.l2 = l2;
-  ra.n_lists = n_chunks;
+  ra.n_lists = n_chunks * HALVES;
   ra.list_len = CAND;
   ra.ids = s->cand_id.as<int32_t>();
   ra.bf_keys = s->cand_key.as<float>();
@@ -771,8 +930,6 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ra.tau = s->tau.as<float>();
   ra.needs = s->needs.as<uint8_t>();
   ra.coll_cap = coll_cap;
-  ra.scratch_id = s->scr_id.as<int32_t>();
-  ra.scratch_key = s->scr_key.as<DF>();
   BF_CUDA(cudaMemsetAsync(s->needs.p, 0, mpad, st), "reset flags");
   rerank_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(ra);
   BF_CUDA(cudaGetLastError(), "rerank (pass A)");
