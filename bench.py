@@ -285,7 +285,7 @@ def brute_force_measure(index, queries, k=10, reps=3):
     flops = 2.0 * len(queries) * n * kp
     res = {"queries": len(queries), "k": k, "ms_end_to_end": round(best * 1e3, 3),
            "qps": round(len(queries) / best), "tensor_tflops": round(flops / best / 1e12, 1),
-           "certified_first_pass": int(st[0]), "second_pass": int(st[1]), "overflow": int(st[2])}
+           "sample_rows": int(st[0]), "max_rows_reranked": int(st[1]), "rescanned": int(st[2])}
     log(f"[bench] brute force: {res}")
     return res
 

@@ -156,13 +156,17 @@ NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* index, const float* queries, int
 
 /* Exact k-NN by scanning every stored vector, the semantics of the reference's sequential
  * search (similarity_search/src/method/seqsearch.cc:143-177), on the tensor cores: a BF16 GEMM
- * (FP32 accumulation) keeps candidates per query, an exact rerank in double-float arithmetic
- * orders them, and a rigorous bound on the BF16 error either certifies the result or triggers a
- * second pass that collects every vector the bound cannot exclude. The ids are the exact top-k
- * (ties by id); distances follow the index's space as the HNSW path reports them (squared L2,
- * 1 - cos on normalised vectors, -dot). dim <= 256, k <= 32. stats (optional, 4 values): queries
- * certified after the first pass, queries resolved by the second pass, queries whose second-pass
- * set overflowed (error), base chunks per query block. Buffer conventions as nmsg_knn_batch. */
+ * (FP32 accumulation) over a sample of the base and an exact rerank in double-float arithmetic
+ * give each query a threshold that, by a rigorous bound on the BF16 error, every true neighbour
+ * reaches; a second BF16 GEMM over the whole base collects the vectors at or above it and the
+ * exact rerank orders them. The ids are the exact top-k (ties by id); distances follow the
+ * index's space as the HNSW path reports them (squared L2, 1 - cos on normalised vectors, -dot).
+ * dim <= 256, k <= 32. The full scan keeps up to 32 vectors per query and per half of a base
+ * chunk; a query that finds more in some chunk is scanned again with a raised threshold (up to
+ * three times), and if it still overflows the call returns NMSG_ERR_CAPACITY (many vectors tied
+ * with the k-th neighbour within the BF16 error bound). stats (optional, 4 values): sample rows
+ * of the first pass, most vectors at or above the threshold for one query, queries rescanned,
+ * base chunks per query block. Buffer conventions as nmsg_knn_batch. */
 NMSG_API int nmsg_bruteforce_knn(nmsg_index* index, const float* queries, int64_t nq, int32_t dim, int32_t k,
                                  int32_t kmax, int32_t* ids, float* dists, int32_t* counts, int64_t* stats,
                                  uint32_t flags, void* stream);

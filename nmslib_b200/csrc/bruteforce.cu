@@ -2,17 +2,19 @@
 // search (similarity_search/src/method/seqsearch.cc:143-177: every stored object is compared
 // with the query and the k best are kept, knnquery.cc:67-75) — computed as:
 //
-//   pass A  a tcgen05 BF16 x BF16 -> FP32 GEMM of 128-query tiles against 256-row base tiles
-//           (TMA-fed, accumulators double-buffered in TMEM) whose epilogue keeps, per query and
-//           per chunk of the base, the C best BF16 scores;
+//   sample  a tcgen05 BF16 x BF16 -> FP32 GEMM of 128-query tiles against a strided sample of
+//           the 256-row base tiles (TMA-fed, accumulators double-buffered in TMEM) whose epilogue
+//           keeps, per query, the C best of the sample's 32-column group maxima (one base
+//           vector per group);
 //   rerank  exact scores of those candidates in double-float arithmetic (error-free products and
-//           sums on FP32 units, about 2^-44 relative), top-k by (distance, id);
-//   certify with a rigorous per-query bound eps on |BF16 score - exact score|: if every chunk's
-//           C-th best BF16 score is below (exact k-th score - eps), no vector outside the
-//           candidates can reach the top k;
-//   pass B  for the queries that are not certified, the same GEMM again, now collecting every
-//           vector whose BF16 score is >= exact k-th score - eps, then the exact rerank of
-//           that set. Queries whose set overflows fall back to an exact scan on CUDA cores.
+//           sums on FP32 units, about 2^-44 relative); the exact k-th score of the sample is a
+//           lower bound of the exact k-th score of the whole base, so with a rigorous per-query
+//           bound eps on |BF16 score - exact score|, tau = (sample k-th - eps) is a BF16 score
+//           that every true top-k vector reaches;
+//   scan    the same GEMM over every base tile, collecting each vector whose BF16 score is
+//           >= tau (a few hundred per query), then the exact rerank of that set. A query whose
+//           set overflows the collection buffer is scanned once more with tau raised to the
+//           exact k-th score of what it did collect less eps (again a lower bound).
 //
 // So the returned ids are the exact top-k (ties by id), independent of BF16 rounding.
 // Scores ("keys", larger is better): negdot and cosine use q.x (queries of the cosine space
@@ -23,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -55,33 +58,36 @@ struct GemmArgs {
   int stages;         // base-tile pipeline depth (3 when kb <= 2, else 2)
   int n;              // base rows
   int nq;             // queries
-  int n_tiles;        // ceil(n / BN)
-  int chunk_tiles;    // base tiles per work item
+  int n_tiles;        // tiles visited: tile j of the scan is base tile j * tile_step
+  int tile_step;      // 1 for the full scan, > 1 for the sample
+  int chunk_tiles;    // visited tiles per work item
   int n_chunks;
   int q_blocks;
   int mode;           // 0: top-CAND per (chunk, column half); 1: collect keys >= tau
-  int key_l2;         // 1: key = 2 dot - |x|^2
-  const float* xnorm2;  // padded to n_tiles * BN
-  float* cand_key;    // [nq][n_chunks * HALVES][CAND]
-  int32_t* cand_id;
+  int per_column;     // mode 0: offer every column, not only each 32-column group's best
+  int key_l2;         // 1: key = 2 dot - |x|^2, 0: key = dot
+  const float* xnorm2;  // |x|^2 (l2) or 0, +inf for the padding rows up to n_tiles * BN
+  // one list of CAND entries per (query, chunk, column half), written only by the thread that
+  // owns that query row in that work item: mode 0 the best group maxima, mode 1 the rows whose
+  // key reaches tau (the count may exceed CAND: the list overflowed)
+  float* list_key;    // [nq][n_chunks * HALVES][CAND]
+  int32_t* list_id;
+  int32_t* list_cnt;  // [nq][n_chunks * HALVES]
   const float* tau;   // [nq]
   const uint8_t* q_active;  // [q_blocks * BM]
-  int32_t* coll_id;   // [nq][coll_cap]
-  float* coll_key;
-  int32_t* coll_cnt;  // [nq]
-  int coll_cap;
   int32_t* status;
 };
 
 // Shared memory: Q blocks | base stages | candidate lists | barriers (1024-aligned base).
 struct SmemLayout {
-  int q_off, x_off, key_off, id_off, bar_off, total;
+  int q_off, x_off, key_off, id_off, nrm_off, bar_off, total;
   __host__ __device__ SmemLayout(int kb, int stages) {
     q_off = 0;
     x_off = q_off + kb * Q_BLOCK_BYTES;
     key_off = x_off + stages * X_STAGE_BYTES;
     id_off = key_off + HALVES * BM * LIST_STRIDE * 4;
-    bar_off = (id_off + HALVES * BM * LIST_STRIDE * 4 + 7) & ~7;
+    nrm_off = id_off + HALVES * BM * LIST_STRIDE * 4;  // per epilogue warp: its 128 columns' |x|^2
+    bar_off = (nrm_off + EPI_WARPS * (BN / HALVES) * 4 + 7) & ~7;
     total = bar_off + 8 * (2 * 4 + 2 + 4) + 16;
   }
 };
@@ -92,6 +98,12 @@ __device__ __forceinline__ bool item_active(const GemmArgs& a, int qb) {
   for (int i = 0; i < BM; ++i)
     if (p[i]) return true;
   return false;
+}
+
+// First active work item at or after `item` in this CTA's round-robin sequence (n_items if none).
+__device__ __forceinline__ int next_active_item(const GemmArgs& a, int item, int n_items) {
+  while (item < n_items && !item_active(a, item % a.q_blocks)) item += gridDim.x;
+  return item;
 }
 
 // A row's candidate list is a min-heap of CAND (key, column) pairs in shared memory: the root is
@@ -139,6 +151,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint8_t* sx = base + L.x_off;
   float* skey = reinterpret_cast<float*>(base + L.key_off);
   int32_t* sid = reinterpret_cast<int32_t*>(base + L.id_off);
+  float* snrm = reinterpret_cast<float*>(base + L.nrm_off);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + L.bar_off);
   uint64_t* x_full = bars;          // [4]
   uint64_t* x_empty = bars + 4;     // [4]
@@ -177,20 +190,29 @@ __global__ void __launch_bounds__(kThreads, 1)
       prefetch_tmap(&tmx);
       int stage = 0;
       uint32_t xphase = 0, qphase = 0;
-      int done_items = 0;
-      for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
-        const int qb = item / a.n_chunks, chunk = item % a.n_chunks;
-        if (!item_active(a, qb)) continue;
-        if (done_items > 0) {
-          ok = mbar_wait(q_empty, qphase);
-          qphase ^= 1;
+      int prev_qb = -1;
+      // items are chunk-major: the CTAs running at the same time read the same base chunk, which
+      // stays in L2 while every query block passes over it. The query block is loaded only when
+      // it differs from the previous item's (for batches of <= 128 queries, once per CTA).
+      for (int item = next_active_item(a, blockIdx.x, n_items); item < n_items && ok;
+           item = next_active_item(a, item + gridDim.x, n_items)) {
+        const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
+        if (qb != prev_qb) {
+          if (prev_qb >= 0) {
+            ok = mbar_wait(q_empty, qphase);
+            qphase ^= 1;
+            if (!ok) break;
+          }
+          mbar_arrive_expect_tx(q_full, a.kb * Q_BLOCK_BYTES);
+          for (int kb = 0; kb < a.kb; ++kb) tma_load_2d(sq + kb * Q_BLOCK_BYTES, &tmq, q_full, kb * BK, qb * BM);
+          prev_qb = qb;
         }
-        mbar_arrive_expect_tx(q_full, a.kb * Q_BLOCK_BYTES);
-        for (int kb = 0; kb < a.kb; ++kb) tma_load_2d(sq + kb * Q_BLOCK_BYTES, &tmq, q_full, kb * BK, qb * BM);
         const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
-        for (int t = t0; t < t1 && ok; ++t) {
+        for (int vt = t0; vt < t1 && ok; ++vt) {
+          const int t = vt * a.tile_step;
           for (int kb = 0; kb < a.kb && ok; ++kb) {
             ok = mbar_wait(&x_empty[stage], xphase ^ 1);
+            if (!ok) break;
             mbar_arrive_expect_tx(&x_full[stage], X_STAGE_BYTES);
             tma_load_2d(sx + stage * X_STAGE_BYTES, &tmx, &x_full[stage], kb * BK, t * BN);
             if (++stage == stages) {
@@ -199,7 +221,6 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
           }
         }
-        ++done_items;
       }
     }
   } else if (warp == EPI_WARPS + 1) {
@@ -209,15 +230,18 @@ __global__ void __launch_bounds__(kThreads, 1)
       int stage = 0;
       uint32_t xphase = 0, qphase = 0;
       uint32_t accphase[2] = {0, 0};
-      int tcount = 0;
-      for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
-        const int qb = item / a.n_chunks, chunk = item % a.n_chunks;
-        if (!item_active(a, qb)) continue;
-        ok = mbar_wait(q_full, qphase);
-        qphase ^= 1;
-        tc_fence_after();
+      int tcount = 0, prev_qb = -1;
+      for (int item = next_active_item(a, blockIdx.x, n_items); item < n_items && ok;) {
+        const int next = next_active_item(a, item + gridDim.x, n_items);
+        const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
+        if (qb != prev_qb) {
+          ok = mbar_wait(q_full, qphase);
+          qphase ^= 1;
+          tc_fence_after();
+          prev_qb = qb;
+        }
         const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
-        for (int t = t0; t < t1 && ok; ++t, ++tcount) {
+        for (int vt = t0; vt < t1 && ok; ++vt, ++tcount) {
           const int buf = tcount & 1;
           ok = mbar_wait(&acc_empty[buf], accphase[buf] ^ 1);
           accphase[buf] ^= 1;
@@ -238,95 +262,133 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           umma_commit(&acc_full[buf]);
         }
-        umma_commit(q_empty);
+        // the query block's buffer is free for the next one once these MMAs complete
+        if (next < n_items && next % a.q_blocks != qb) umma_commit(q_empty);
+        item = next;
       }
     }
   } else {
     // ------------------------------------------------ epilogue: warps 0-7; thread = one query row
-    // (TMEM lane) for one half of the tile's columns
+    // (TMEM lane) for one half of the tile's columns, 32 columns at a time
     const int quarter = warp & 3, half = warp >> 2;
     const int row = quarter * 32 + lane;
     float* lk = skey + (half * BM + row) * LIST_STRIDE;
     int32_t* li = sid + (half * BM + row) * LIST_STRIDE;
+    float* snw = snrm + warp * (BN / HALVES);  // |x|^2 of this warp's 128 columns of the tile
     uint32_t accphase[2] = {0, 0};
     int tcount = 0;
     for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
-      const int qb = item / a.n_chunks, chunk = item % a.n_chunks;
+      const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
       if (!item_active(a, qb)) continue;
       const int q = qb * BM + row;
       const bool qvalid = q < a.nq;
       float thr = -INFINITY;  // mode 0: the list's smallest key once full; mode 1: tau
       int nfill = 0;
-      if (a.mode == 1) thr = (qvalid && a.q_active[q]) ? a.tau[q] : INFINITY;
+      // mode 1: a finite floor, so the -inf keys of columns past the last row never qualify
+      if (a.mode == 1) thr = (qvalid && a.q_active[q]) ? fmaxf(a.tau[q], -FLT_MAX) : INFINITY;
       const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
-      // |x|^2 of this half's 128 columns, 4 per lane, loaded one tile ahead and handed to the
-      // other lanes by shuffles
+      // |x|^2 of this half's 128 columns, 4 per lane, loaded one tile ahead
       const float4* xn4 = reinterpret_cast<const float4*>(a.xnorm2) + half * (BN / HALVES / 4) + lane;
       float4 nrm_next = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (a.key_l2 && t0 < t1) nrm_next = __ldg(xn4 + (size_t)t0 * (BN / 4));
-      for (int t = t0; t < t1 && ok; ++t, ++tcount) {
+      if (t0 < t1) nrm_next = __ldg(xn4 + (size_t)t0 * a.tile_step * (BN / 4));
+      const float ks = a.key_l2 ? 2.0f : 1.0f;
+      const size_t list = ((size_t)q * a.n_chunks + chunk) * HALVES + half;
+      int32_t* cid = a.list_id + list * CAND;
+      float* ckey = a.list_key + list * CAND;
+      int ncoll = 0;
+      for (int vt = t0; vt < t1 && ok; ++vt, ++tcount) {
+        const int t = vt * a.tile_step;
         const int buf = tcount & 1;
-        const float4 nrm = nrm_next;
-        if (a.key_l2 && t + 1 < t1) nrm_next = __ldg(xn4 + (size_t)(t + 1) * (BN / 4));
+        __syncwarp();  // every lane is done with the previous tile's norms
+        reinterpret_cast<float4*>(snw)[lane] = nrm_next;
+        if (vt + 1 < t1) nrm_next = __ldg(xn4 + (size_t)(t + a.tile_step) * (BN / 4));
+        __syncwarp();
         ok = mbar_wait(&acc_full[buf], accphase[buf]);
         accphase[buf] ^= 1;
         tc_fence_after();
+        // TMEM loads of the next group of 32 columns overlap the work on the current one
+        const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + buf * BN + half * (BN / HALVES);
+        uint32_t ra[32];
+        tmem_ld32_issue(tb, ra);
+        tmem_ld_wait(ra);
 #pragma unroll 1
-        for (int c = 0; c < BN / 32 / HALVES; ++c) {
-          const int ccol = half * (BN / HALVES) + c * 32;  // column inside the tile
+        for (int c = 0; c < BN / HALVES / 32; ++c) {
+          uint32_t cur[32];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) cur[i] = ra[i];
+          if (c + 1 < BN / HALVES / 32) {
+            tmem_ld32_issue(tb + 32 * (c + 1), ra);
+          } else {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[buf]);  // the accumulator is read out
+          }
+          const int col0 = t * BN + half * (BN / HALVES) + c * 32;
+          // keys: ks * acc - xnorm2 (l2: 2 q.x - |x|^2, where 2 acc is exact so one FMA rounds
+          // as the two-step form would; dot spaces: acc - 0). Rows past the base have
+          // xnorm2 = +inf, so their key is -inf.
           float v[32];
-          tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + buf * BN + ccol, v);
-          const int col0 = t * BN + ccol;
-          // keys of all 32 columns without branches (independent, so they overlap), then one
-          // test of their maximum against the threshold; the per-column path runs only if it passes
-          if (a.key_l2) {
+          const float4* nv = reinterpret_cast<const float4*>(snw + c * 32);
 #pragma unroll
-            for (int i = 0; i < 32; ++i) {
-              const float comp = (i & 3) == 0 ? nrm.x : (i & 3) == 1 ? nrm.y : (i & 3) == 2 ? nrm.z : nrm.w;
-              const float xn = __shfl_sync(0xffffffffu, comp, c * 8 + (i >> 2));
-              v[i] = __fsub_rn(__fmul_rn(2.0f, v[i]), xn);
-            }
+          for (int j = 0; j < 8; ++j) {
+            const float4 x4 = nv[j];  // same address in every lane: a broadcast
+            v[4 * j + 0] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 0]), -x4.x);
+            v[4 * j + 1] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 1]), -x4.y);
+            v[4 * j + 2] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 2]), -x4.z);
+            v[4 * j + 3] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 3]), -x4.w);
           }
-          if (col0 + 32 > a.n) {
+          float m[16];
 #pragma unroll
-            for (int i = 0; i < 32; ++i)
-              if (col0 + i >= a.n) v[i] = -INFINITY;
-          }
-          float mx = v[0];
+          for (int i = 0; i < 16; ++i) m[i] = fmaxf(v[i], v[i + 16]);
 #pragma unroll
-          for (int i = 1; i < 32; ++i) mx = fmaxf(mx, v[i]);
-          if (a.mode == 0) {
-            if (mx > thr || nfill < CAND) {
+          for (int w = 8; w > 0; w >>= 1)
 #pragma unroll
+            for (int i = 0; i < w; ++i) m[i] = fmaxf(m[i], m[i + w]);
+          const float mx = m[0];
+          if (a.mode == 0 && a.per_column) {
+            // small bases (the sample is all of it): every column is offered
+            if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
+              float vl[32];
+#pragma unroll
+              for (int i = 0; i < 32; ++i) vl[i] = v[i];
+#pragma unroll 1
               for (int i = 0; i < 32; ++i)
-                if (v[i] > thr || nfill < CAND) {
-                  if (col0 + i < a.n) list_offer(lk, li, nfill, thr, v[i], col0 + i);
-                }
+                if ((vl[i] > thr || nfill < CAND) && vl[i] > -INFINITY) list_offer(lk, li, nfill, thr, vl[i], col0 + i);
+            }
+          } else if (a.mode == 0) {
+            // the group's best column is the candidate: the lists hold distinct base vectors,
+            // so the exact k-th key among them still bounds the true k-th key from below
+            if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
+              int arg = 31;
+#pragma unroll
+              for (int i = 30; i >= 0; --i) arg = v[i] == mx ? i : arg;
+              list_offer(lk, li, nfill, thr, mx, col0 + arg);
             }
           } else if (mx >= thr) {
+            // plain stores into this row's own list: no atomics, nothing to wait for
 #pragma unroll
             for (int i = 0; i < 32; ++i)
               if (v[i] >= thr) {
-                const int slot = atomicAdd(a.coll_cnt + q, 1);
-                if (slot < a.coll_cap) {
-                  a.coll_id[(size_t)q * a.coll_cap + slot] = col0 + i;
-                  a.coll_key[(size_t)q * a.coll_cap + slot] = v[i];
+                if (ncoll < CAND) {
+                  cid[ncoll] = col0 + i;
+                  ckey[ncoll] = v[i];
                 }
+                ++ncoll;
               }
           }
+          __syncwarp();
+          if (c + 1 < BN / HALVES / 32) tmem_ld_wait(ra);
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[buf]);
       }
-      if (a.mode == 0 && qvalid) {
-        const size_t list = (size_t)q * a.n_chunks * HALVES + chunk * HALVES + half;
-        float* ok_out = a.cand_key + list * CAND;
-        int32_t* oi_out = a.cand_id + list * CAND;
-        for (int j = 0; j < CAND; ++j) {
-          ok_out[j] = j < nfill ? lk[j] : -INFINITY;
-          oi_out[j] = j < nfill ? li[j] : -1;
+      if (qvalid) {
+        if (a.mode == 0) {
+          for (int j = 0; j < nfill; ++j) {
+            ckey[j] = lk[j];
+            cid[j] = li[j];
+          }
+          ncoll = nfill;
         }
+        a.list_cnt[list] = ncoll;
       }
     }
   }
@@ -359,42 +421,25 @@ __device__ __forceinline__ DF df_mul_ff(float a, float b) {
 }
 __device__ __forceinline__ bool df_greater(DF a, DF b) { return a.hi > b.hi || (a.hi == b.hi && a.lo > b.lo); }
 
-// Exact-ish key of one (query, row) pair, warp-cooperative over the dimension.
-__device__ DF exact_key(const float* q, const float* x, int dim, bool l2, DF xnorm) {
-  const int lane = threadIdx.x & 31;
-  DF acc{0.0f, 0.0f};
-  for (int e = lane; e < dim; e += 32) acc = df_add_df(acc, df_mul_ff(q[e], x[e]));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    DF other{__shfl_xor_sync(0xffffffffu, acc.hi, o), __shfl_xor_sync(0xffffffffu, acc.lo, o)};
-    acc = df_add_df(acc, other);
-  }
-  if (l2) {
-    DF two{__fmul_rn(2.0f, acc.hi), __fmul_rn(2.0f, acc.lo)};
-    DF neg{-xnorm.hi, -xnorm.lo};
-    return df_add_df(two, neg);
-  }
-  return acc;
-}
-
 struct RerankArgs {
   const float* q;        // [nq][dim] (normalised for cosine)
   const float* x;        // [n][dim] natural order, fp32
   const float* xn_hi;    // l2: |x|^2 as double-float
   const float* xn_lo;
   int dim, n, nq, k, l2;
-  int n_lists, list_len;       // pass A: candidate lists per query and their length
-  const int32_t* ids;          // pass A: [nq][n_lists * list_len] (-1 = empty); pass B: [nq][coll_cap]
-  const float* bf_keys;        // BF16 keys, same layout
-  const int32_t* list_count;   // pass B: per-query count (null in pass A)
+  int n_lists;                 // lists of CAND entries per query
+  int32_t* ids;                // [nq][n_lists][CAND] internal ids, compacted in place here
+  float* bf_keys;              // BF16 keys, same layout
+  const int32_t* list_count;   // [nq][n_lists] entries found per list (more than CAND: overflow)
   const float* eps;            // [nq] bound on |BF16 key - exact key|
-  int coll_cap;
+  const uint8_t* only;         // optional: rerank only the queries flagged here
   // outputs
   int32_t* out_ids;            // [nq][k] internal ids, best first
   DF* out_keys;                // [nq][k]
   int32_t* out_count;          // [nq]
-  float* tau;                  // pass A: [nq] threshold for the second pass
-  uint8_t* needs;              // pass A: 1 = not certified; pass B: 1 = collection overflowed
+  float* tau;                  // [nq] BF16 threshold that every true top-k vector reaches
+  uint8_t* needs;              // optional [nq]: 1 = some list overflowed
+  int32_t* found;              // optional [nq]: entries found over all lists
 };
 
 // (key, id) order of the result: larger key first, then smaller id.
@@ -417,33 +462,52 @@ __device__ DF exact_key_lane(const float* __restrict__ q, const float* __restric
 //     at or above B_k all have exact keys >= B_k - eps, anything below B_k - 2 eps has an exact
 //     key < B_k - eps), so only they get exact keys, one candidate per lane;
 //  3. the exact top k by (key desc, id asc), merged 32 candidates at a time;
-//  4. pass A: the certificate and the second-pass threshold.
+//  4. tau = exact k-th key - eps (rounded down, less one ulp of the double-float's high part):
+//     the candidates are real base vectors, so their exact k-th key is at most the true k-th
+//     key, and every true top-k vector has a BF16 key >= tau.
 __global__ void rerank_kernel(RerankArgs a) {
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (q >= a.nq) return;
-  const bool pass_b = a.list_count != nullptr;
-  int total = pass_b ? min(a.list_count[q], a.coll_cap) : a.n_lists * a.list_len;
-  const size_t base = pass_b ? (size_t)q * a.coll_cap : (size_t)q * a.n_lists * a.list_len;
-  const int32_t* ids = a.ids + base;
-  const float* bk = a.bf_keys + base;
+  if (a.only && !a.only[q]) return;
+  const size_t base = (size_t)q * a.n_lists * CAND;
+  int32_t* ids = a.ids + base;
+  float* bk = a.bf_keys + base;
   const float eps = a.eps[q];
 
-  // pass A: every full list bounds the vectors it dropped by its smallest key
-  float worst_bf_list = -INFINITY;
-  if (!pass_b) {
-    for (int c = 0; c < a.n_lists; ++c) {
-      float mn = INFINITY;
-      bool full = true;
-      for (int j = lane; j < a.list_len; j += 32) {
-        full &= ids[c * a.list_len + j] >= 0;
-        mn = fminf(mn, bk[c * a.list_len + j]);
+  // 0. compact the lists in place: list l's first min(count, CAND) entries move to the running
+  //    total (never past their own position, and each lane reads before any lane writes)
+  int total = 0, found_all = 0;
+  bool overflow = false;
+  const int32_t* lc = a.list_count + (size_t)q * a.n_lists;
+  for (int l0 = 0; l0 < a.n_lists; l0 += 32) {
+    const int my_cnt = l0 + lane < a.n_lists ? lc[l0 + lane] : 0;
+    found_all += my_cnt;
+    overflow |= my_cnt > CAND;
+    unsigned nonempty = __ballot_sync(0xffffffffu, my_cnt > 0);
+    while (nonempty) {
+      const int j = __ffs(nonempty) - 1;
+      nonempty &= nonempty - 1;
+      const int cnt = min(__shfl_sync(0xffffffffu, my_cnt, j), CAND);
+      const int src = (l0 + j) * CAND + lane;
+      int32_t id = 0;
+      float key = 0.0f;
+      if (lane < cnt) {
+        id = ids[src];
+        key = bk[src];
       }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-      if (__all_sync(0xffffffffu, full)) worst_bf_list = fmaxf(worst_bf_list, mn);
+      __syncwarp();
+      if (lane < cnt) {
+        ids[total + lane] = id;
+        bk[total + lane] = key;
+      }
+      __syncwarp();
+      total += cnt;
     }
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) found_all += __shfl_xor_sync(0xffffffffu, found_all, o);
+  overflow = __any_sync(0xffffffffu, overflow);
 
   // 1. k-th largest BF16 key (pairs ordered by key desc, slot asc)
   float prev_k = INFINITY;
@@ -453,7 +517,6 @@ __global__ void rerank_kernel(RerankArgs a) {
     float bkey = -INFINITY;
     int bslot = 0x7fffffff;
     for (int t = lane; t < total; t += 32) {
-      if (ids[t] < 0) continue;
       const float kv = bk[t];
       const bool below = kv < prev_k || (kv == prev_k && t > prev_s);  // after the previous pick
       if (below && (kv > bkey || (kv == bkey && t < bslot))) {
@@ -487,7 +550,7 @@ __global__ void rerank_kernel(RerankArgs a) {
     int id = -1;
     if (t < total) {
       id = ids[t];
-      if (id >= 0 && !(bk[t] >= cut)) id = -1;
+      if (!(bk[t] >= cut)) id = -1;
     }
     if (__ballot_sync(0xffffffffu, id >= 0) == 0) continue;
     DF key{-INFINITY, 0.0f};
@@ -553,16 +616,9 @@ __global__ void rerank_kernel(RerankArgs a) {
   const float kth = __shfl_sync(0xffffffffu, top_k.hi, kk - 1);
   if (lane == 0) {
     a.out_count[q] = have;
-    if (!pass_b) {
-      // every vector outside the lists has BF16 key <= worst_bf_list, so exact key <=
-      // worst_bf_list + eps; certified when that is below the k-th exact key (less half an ulp)
-      const float tau = have == kk ? __fsub_rd(__fsub_rd(kth, eps), fabsf(kth) * 1.1920929e-7f) : -INFINITY;
-      const bool cert = have == a.n || (have == kk && worst_bf_list < tau);
-      a.tau[q] = tau;
-      a.needs[q] = cert ? 0 : 1;
-    } else {
-      a.needs[q] = a.list_count[q] > a.coll_cap ? 1 : 0;
-    }
+    a.tau[q] = have == kk ? __fsub_rd(__fsub_rd(kth, eps), fabsf(kth) * 1.1920929e-7f) : -INFINITY;
+    if (a.needs) a.needs[q] = overflow ? 1 : 0;
+    if (a.found) a.found[q] = found_all;
   }
 }
 
@@ -578,7 +634,7 @@ struct BruteForceState {
   int kp = 0;       // padded dim (multiple of 64, <= 256)
   float max_xn = 0; // largest |x|^2 over the base (l2 bound)
   DevBuf x16, x32, xn, xn_hi, xn_lo, xt_max, dx_max;
-  DevBuf q32, q16, qn_hi, qn_lo, eps, cand_key, cand_id, tau, needs, qact, coll_id, coll_key, coll_cnt;
+  DevBuf q32, q16, qn_hi, qn_lo, eps, cand_key, cand_id, cand_cnt, tau, needs, qact, coll_id, coll_key, coll_cnt, found;
   DevBuf out_id, out_key, out_cnt, scr_id, scr_key, fin_id, fin_key, fin_cnt, status;
   DevBuf h_q, h_ids, h_dists, h_counts;
   CUtensorMap tmx;
@@ -587,8 +643,8 @@ struct BruteForceState {
 void destroy_bruteforce(BruteForceState* s) {
   if (!s) return;
   for (DevBuf* b : {&s->x16, &s->x32, &s->xn, &s->xn_hi, &s->xn_lo, &s->xt_max, &s->dx_max, &s->q32, &s->q16, &s->qn_hi,
-                    &s->qn_lo, &s->eps, &s->cand_key, &s->cand_id, &s->tau, &s->needs, &s->qact, &s->coll_id,
-                    &s->coll_key, &s->coll_cnt, &s->out_id, &s->out_key, &s->out_cnt, &s->scr_id, &s->scr_key,
+                    &s->qn_lo, &s->eps, &s->cand_key, &s->cand_id, &s->cand_cnt, &s->tau, &s->needs, &s->qact,
+                    &s->coll_id, &s->coll_key, &s->coll_cnt, &s->found, &s->out_id, &s->out_key, &s->out_cnt, &s->scr_id, &s->scr_key,
                     &s->fin_id, &s->fin_key, &s->fin_cnt, &s->status, &s->h_q, &s->h_ids, &s->h_dists, &s->h_counts})
     b->release();
   delete s;
@@ -599,7 +655,7 @@ namespace {
 // bf16 copy of the base (row pitch kp, zero padded), |x|^2 in fp32 and double-float, and the
 // per-dimension maxima of |bf16(x)| and |x - bf16(x)| (as float bits, non-negative, so integer
 // max is float max). One warp per row.
-__global__ void prep_base_kernel(const float* __restrict__ x, int64_t n, int dim, int kp, __nv_bfloat16* __restrict__ x16,
+__global__ void prep_base_kernel(const float* __restrict__ x, int64_t n, int dim, int kp, int l2, __nv_bfloat16* __restrict__ x16,
                                  float* __restrict__ xn, float* __restrict__ xn_hi, float* __restrict__ xn_lo,
                                  unsigned* __restrict__ xt_max, unsigned* __restrict__ dx_max) {
   const int lane = threadIdx.x & 31;
@@ -624,7 +680,7 @@ __global__ void prep_base_kernel(const float* __restrict__ x, int64_t n, int dim
     acc = df_add_df(acc, other);
   }
   if (lane == 0) {
-    xn[row] = acc.hi;  // fp32 |x|^2 used with the BF16 scores (its error is part of eps)
+    xn[row] = l2 ? acc.hi : 0.0f;  // fp32 |x|^2 used with the BF16 scores (its error is part of eps)
     xn_hi[row] = acc.hi;
     xn_lo[row] = acc.lo;
   }
@@ -694,19 +750,16 @@ __global__ void prep_query_kernel(const float* __restrict__ qin, int nq, int dim
 }
 
 // Final rows: external ids and distances in the index's space convention.
-__global__ void finish_kernel(const int32_t* __restrict__ id_a, const DF* __restrict__ key_a,
-                              const int32_t* __restrict__ cnt_a, const int32_t* __restrict__ id_b,
-                              const DF* __restrict__ key_b, const int32_t* __restrict__ cnt_b,
-                              const uint8_t* __restrict__ use_b, int nq, int k, int kmax, int space,
+__global__ void finish_kernel(const int32_t* __restrict__ id_in, const DF* __restrict__ key_in,
+                              const int32_t* __restrict__ cnt_in, int nq, int k, int kmax, int space,
                               const float* __restrict__ qn_hi, const float* __restrict__ qn_lo,
                               const int32_t* __restrict__ ext_id, int32_t* __restrict__ ids, float* __restrict__ dists,
                               int32_t* __restrict__ counts) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nq) return;
-  const bool b = use_b && use_b[q];
-  const int32_t* id = (b ? id_b : id_a) + (size_t)q * k;
-  const DF* key = (b ? key_b : key_a) + (size_t)q * k;
-  const int cnt = b ? cnt_b[q] : cnt_a[q];
+  const int32_t* id = id_in + (size_t)q * k;
+  const DF* key = key_in + (size_t)q * k;
+  const int cnt = cnt_in[q];
   for (int j = 0; j < kmax; ++j) {
     if (j < cnt && j < k) {
       ids[(size_t)q * kmax + j] = ext_id[id[j]];
@@ -797,9 +850,13 @@ int prepare_base(nmsg_index* h, BruteForceState* s) {
   BF_CUDA(s->dx_max.ensure(dim * 4, true), "cudaMalloc(bounds)");
   const int wpb = 8;
   prep_base_kernel<<<(unsigned)((n + wpb - 1) / wpb), 32 * wpb>>>(
-      s->x32.as<float>(), n, dim, s->kp, s->x16.as<__nv_bfloat16>(), s->xn.as<float>(), s->xn_hi.as<float>(),
+      s->x32.as<float>(), n, dim, s->kp, h->space == NMSG_SPACE_L2, s->x16.as<__nv_bfloat16>(), s->xn.as<float>(), s->xn_hi.as<float>(),
       s->xn_lo.as<float>(), s->xt_max.as<unsigned>(), s->dx_max.as<unsigned>());
   BF_CUDA(cudaGetLastError(), "prepare base");
+  if (npad > n) {
+    const std::vector<float> inf((size_t)(npad - n), INFINITY);
+    BF_CUDA(cudaMemcpy(s->xn.as<float>() + n, inf.data(), inf.size() * 4, cudaMemcpyHostToDevice), "pad norms");
+  }
   BF_CUDA(cudaDeviceSynchronize(), "prepare base");
   if (!make_tmap(&s->tmx, s->x16.p, n, s->kp, BN)) return bf_fail(NMSG_ERR_DEVICE, "cuTensorMapEncodeTiled (base)");
   return NMSG_OK;
@@ -849,11 +906,33 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   const int q_blocks = (int)((nq + BM - 1) / BM);
   const int mpad = q_blocks * BM;
   const int n_tiles = (int)((n + BN - 1) / BN);
-  int n_chunks = std::max(1, std::min(n_tiles, (4 * h->num_sms + q_blocks - 1) / q_blocks));
-  const int chunk_tiles = (n_tiles + n_chunks - 1) / n_chunks;
-  n_chunks = (n_tiles + chunk_tiles - 1) / chunk_tiles;
-  const int n_items = q_blocks * n_chunks;
-  const int coll_cap = 16384;
+
+  // the sample: every tile_step-th base tile, at least 16 tiles (or all of them), about 1/16
+  // of the base; split into chunks so the sample pass also fills the GPU for small batches
+  const int s_tiles = std::min(n_tiles, std::max(16, n_tiles / 16));
+  const int s_step = n_tiles / s_tiles;
+  int s_chunks = std::max(1, std::min(s_tiles / 4, h->num_sms / q_blocks));
+  const int s_chunk_tiles = (s_tiles + s_chunks - 1) / s_chunks;
+  s_chunks = (s_tiles + s_chunk_tiles - 1) / s_chunk_tiles;
+  // the full scan: about 8 or more work items per CTA, the split whose busiest CTA carries the
+  // least excess over the average (items are dealt round-robin)
+  int chunk_tiles = n_tiles, n_chunks = 1;
+  {
+    const int lo = std::max(1, std::min(n_tiles, (8 * h->num_sms + q_blocks - 1) / q_blocks));
+    const int hi = std::min(n_tiles, 2 * lo);
+    double best = 1e30;
+    for (int c = lo; c <= hi; ++c) {
+      const int ct = (n_tiles + c - 1) / c, cc = (n_tiles + ct - 1) / ct;
+      const int64_t items = (int64_t)q_blocks * cc;
+      const int64_t rounds = (items + h->num_sms - 1) / h->num_sms;
+      const double cost = (double)rounds * ct / ((double)q_blocks * n_tiles / h->num_sms);
+      if (cost < best - 1e-9) {
+        best = cost;
+        chunk_tiles = ct;
+        n_chunks = cc;
+      }
+    }
+  }
 
   // inputs
   const float* qin = queries;
@@ -867,13 +946,23 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   BF_CUDA(s->qn_hi.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->qn_lo.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->eps.ensure(nq * 4, false), "cudaMalloc");
-  BF_CUDA(s->cand_key.ensure((size_t)nq * n_chunks * HALVES * CAND * 4, false), "cudaMalloc");
-  BF_CUDA(s->cand_id.ensure((size_t)nq * n_chunks * HALVES * CAND * 4, false), "cudaMalloc");
+  const size_t s_lists = (size_t)nq * s_chunks * HALVES, c_lists = (size_t)nq * n_chunks * HALVES;
+  BF_CUDA(s->cand_key.ensure(s_lists * CAND * 4, false), "cudaMalloc");
+  BF_CUDA(s->cand_id.ensure(s_lists * CAND * 4, false), "cudaMalloc");
+  BF_CUDA(s->cand_cnt.ensure(s_lists * 4, false), "cudaMalloc");
   BF_CUDA(s->tau.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->needs.ensure(mpad, false), "cudaMalloc");
+  BF_CUDA(s->qact.ensure(mpad, false), "cudaMalloc");
   BF_CUDA(s->out_id.ensure((size_t)nq * k * 4, false), "cudaMalloc");
   BF_CUDA(s->out_key.ensure((size_t)nq * k * 8, false), "cudaMalloc");
   BF_CUDA(s->out_cnt.ensure(nq * 4, false), "cudaMalloc");
+  BF_CUDA(s->fin_id.ensure((size_t)nq * k * 4, false), "cudaMalloc");
+  BF_CUDA(s->fin_key.ensure((size_t)nq * k * 8, false), "cudaMalloc");
+  BF_CUDA(s->fin_cnt.ensure(nq * 4, false), "cudaMalloc");
+  BF_CUDA(s->coll_id.ensure(c_lists * CAND * 4, false), "cudaMalloc(collection)");
+  BF_CUDA(s->coll_key.ensure(c_lists * CAND * 4, false), "cudaMalloc(collection)");
+  BF_CUDA(s->coll_cnt.ensure(c_lists * 4, false), "cudaMalloc(collection)");
+  BF_CUDA(s->found.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->status.ensure(4, true), "cudaMalloc");
   const float max_xn = s->max_xn;
   prep_query_kernel<<<(mpad + 7) / 8, 256, 0, st>>>(qin, (int)nq, dim, kp, mpad, cosine, l2, s->xt_max.as<unsigned>(),
@@ -885,30 +974,35 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   if (!make_tmap(&tmq, s->q16.p, mpad, kp, BM)) return bf_fail(NMSG_ERR_DEVICE, "cuTensorMapEncodeTiled (queries)");
   BF_CUDA(cudaMemsetAsync(s->status.p, 0, 4, st), "reset status");
 
+  // 1. top-CAND BF16 candidates of the sample, exact rerank -> tau
   GemmArgs ga;
+  std::memset(&ga, 0, sizeof(ga));
   ga.kb = kb;
   ga.n = (int)n;
   ga.nq = (int)nq;
-  ga.n_tiles = n_tiles;
-  ga.chunk_tiles = chunk_tiles;
-  ga.n_chunks = n_chunks;
+  ga.n_tiles = s_tiles;
+  ga.tile_step = s_step;
+  ga.chunk_tiles = s_chunk_tiles;
+  ga.n_chunks = s_chunks;
   ga.q_blocks = q_blocks;
   ga.stages = kb <= 2 ? 3 : 2;
   ga.mode = 0;
+  ga.per_column = s_tiles == n_tiles;
   ga.key_l2 = l2;
   ga.xnorm2 = s->xn.as<float>();
-  ga.cand_key = s->cand_key.as<float>();
-  ga.cand_id = s->cand_id.as<int32_t>();
+  ga.list_key = s->cand_key.as<float>();
+  ga.list_id = s->cand_id.as<int32_t>();
+  ga.list_cnt = s->cand_cnt.as<int32_t>();
   ga.tau = s->tau.as<float>();
-  ga.q_active = s->needs.as<uint8_t>();
+  ga.q_active = s->qact.as<uint8_t>();
   ga.status = s->status.as<int32_t>();
   const int smem = SmemLayout(kb, ga.stages).total + 1024;
   BF_CUDA(cudaFuncSetAttribute(bf16_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
-  const int grid = std::min(n_items, h->num_sms);
-  bf16_scan_kernel<<<grid, kThreads, smem, st>>>(tmq, s->tmx, ga);
-  BF_CUDA(cudaGetLastError(), "brute-force scan (pass A)");
+  bf16_scan_kernel<<<std::min(q_blocks * s_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, ga);
+  BF_CUDA(cudaGetLastError(), "brute-force scan (sample)");
 
   RerankArgs ra;
+  std::memset(&ra, 0, sizeof(ra));
   ra.q = s->q32.as<float>();
   ra.x = s->x32.as<float>();
   ra.xn_hi = s->xn_hi.as<float>();
@@ -918,61 +1012,71 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ra.nq = (int)nq;
   ra.k = k;
   ra.l2 = l2;
-  ra.n_lists = n_chunks * HALVES;
-  ra.list_len = CAND;
+  ra.n_lists = s_chunks * HALVES;
   ra.ids = s->cand_id.as<int32_t>();
   ra.bf_keys = s->cand_key.as<float>();
-  ra.list_count = nullptr;
+  ra.list_count = s->cand_cnt.as<int32_t>();
   ra.eps = s->eps.as<float>();
   ra.out_ids = s->out_id.as<int32_t>();
   ra.out_keys = s->out_key.as<DF>();
   ra.out_count = s->out_cnt.as<int32_t>();
   ra.tau = s->tau.as<float>();
-  ra.needs = s->needs.as<uint8_t>();
-  ra.coll_cap = coll_cap;
-  BF_CUDA(cudaMemsetAsync(s->needs.p, 0, mpad, st), "reset flags");
-  rerank_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(ra);
-  BF_CUDA(cudaGetLastError(), "rerank (pass A)");
+  const unsigned rr_blocks = (unsigned)((nq + 7) / 8);
+  rerank_kernel<<<rr_blocks, 256, 0, st>>>(ra);
+  BF_CUDA(cudaGetLastError(), "rerank (sample)");
 
-  // which queries are not certified?
-  std::vector<uint8_t> needs(nq);
-  BF_CUDA(cudaMemcpyAsync(needs.data(), s->needs.p, nq, cudaMemcpyDeviceToHost, st), "copy flags");
+  // 2. every base tile, collecting BF16 keys >= tau; exact rerank of the collection. A query
+  //    whose collection overflowed is scanned again with the raised tau of what it collected
+  //    (up to three times: tau rises each time unless the collected keys are all tied).
+  GemmArgs gb = ga;
+  gb.mode = 1;
+  gb.per_column = 0;
+  gb.n_tiles = n_tiles;
+  gb.tile_step = 1;
+  gb.chunk_tiles = chunk_tiles;
+  gb.n_chunks = n_chunks;
+  gb.list_key = s->coll_key.as<float>();
+  gb.list_id = s->coll_id.as<int32_t>();
+  gb.list_cnt = s->coll_cnt.as<int32_t>();
+  RerankArgs rb = ra;
+  rb.n_lists = n_chunks * HALVES;
+  rb.ids = s->coll_id.as<int32_t>();
+  rb.bf_keys = s->coll_key.as<float>();
+  rb.list_count = s->coll_cnt.as<int32_t>();
+  rb.out_ids = s->fin_id.as<int32_t>();
+  rb.out_keys = s->fin_key.as<DF>();
+  rb.out_count = s->fin_cnt.as<int32_t>();
+  rb.needs = s->needs.as<uint8_t>();
+  rb.found = s->found.as<int32_t>();
+  BF_CUDA(cudaMemsetAsync(s->qact.p, 1, mpad, st), "reset flags");
+  int64_t max_collected = 0, rescanned = 0, overflow = 0;
+  std::vector<uint8_t> flags_h(nq);
+  std::vector<int32_t> cnt_h(nq);
   int32_t dstatus = 0;
-  BF_CUDA(cudaMemcpyAsync(&dstatus, s->status.p, 4, cudaMemcpyDeviceToHost, st), "copy status");
-  BF_CUDA(cudaStreamSynchronize(st), "brute force pass A");
-  if (dstatus) return bf_fail(dstatus, "brute-force scan reported a device-side error");
-  int64_t n_uncert = 0;
-  for (uint8_t v : needs) n_uncert += v;
-  const bool pass_b = n_uncert > 0;
-  if (pass_b) {
-    BF_CUDA(s->coll_id.ensure((size_t)nq * coll_cap * 4, false), "cudaMalloc(collection)");
-    BF_CUDA(s->coll_key.ensure((size_t)nq * coll_cap * 4, false), "cudaMalloc(collection)");
-    BF_CUDA(s->coll_cnt.ensure(nq * 4, false), "cudaMalloc(collection)");
-    BF_CUDA(s->fin_id.ensure((size_t)nq * k * 4, false), "cudaMalloc");
-    BF_CUDA(s->fin_key.ensure((size_t)nq * k * 8, false), "cudaMalloc");
-    BF_CUDA(s->fin_cnt.ensure(nq * 4, false), "cudaMalloc");
-    BF_CUDA(s->qact.ensure(mpad, false), "cudaMalloc");
+  constexpr int kScans = 4;
+  for (int attempt = 0; attempt < kScans; ++attempt) {
+    BF_CUDA(cudaMemsetAsync(s->found.p, 0, nq * 4, st), "reset counts");
+    BF_CUDA(cudaMemsetAsync(s->needs.p, 0, mpad, st), "reset flags");
+    bf16_scan_kernel<<<std::min(q_blocks * n_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, gb);
+    BF_CUDA(cudaGetLastError(), "brute-force scan");
+    rb.only = attempt == 0 ? nullptr : s->qact.as<uint8_t>();  // the other queries keep their results
+    rerank_kernel<<<rr_blocks, 256, 0, st>>>(rb);
+    BF_CUDA(cudaGetLastError(), "rerank");
+    BF_CUDA(cudaMemcpyAsync(flags_h.data(), s->needs.p, nq, cudaMemcpyDeviceToHost, st), "copy flags");
+    BF_CUDA(cudaMemcpyAsync(cnt_h.data(), s->found.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
+    BF_CUDA(cudaMemcpyAsync(&dstatus, s->status.p, 4, cudaMemcpyDeviceToHost, st), "copy status");
+    BF_CUDA(cudaStreamSynchronize(st), "brute-force scan");
+    if (dstatus) return bf_fail(dstatus, "brute-force scan reported a device-side error");
+    overflow = 0;
+    for (int64_t i = 0; i < nq; ++i) {
+      max_collected = std::max<int64_t>(max_collected, cnt_h[i]);
+      overflow += flags_h[i];
+    }
+    if (!overflow || attempt + 1 == kScans) break;
+    if (attempt == 0) rescanned = overflow;
     BF_CUDA(cudaMemcpyAsync(s->qact.p, s->needs.p, mpad, cudaMemcpyDeviceToDevice, st), "copy flags");
-    BF_CUDA(cudaMemsetAsync(s->coll_cnt.p, 0, nq * 4, st), "reset counts");
-    ga.mode = 1;
-    ga.q_active = s->qact.as<uint8_t>();
-    ga.coll_id = s->coll_id.as<int32_t>();
-    ga.coll_key = s->coll_key.as<float>();
-    ga.coll_cnt = s->coll_cnt.as<int32_t>();
-    ga.coll_cap = coll_cap;
-    bf16_scan_kernel<<<grid, kThreads, smem, st>>>(tmq, s->tmx, ga);
-    BF_CUDA(cudaGetLastError(), "brute-force scan (pass B)");
-    RerankArgs rb = ra;
-    rb.ids = s->coll_id.as<int32_t>();
-    rb.bf_keys = s->coll_key.as<float>();
-    rb.list_count = s->coll_cnt.as<int32_t>();
-    rb.out_ids = s->fin_id.as<int32_t>();
-    rb.out_keys = s->fin_key.as<DF>();
-    rb.out_count = s->fin_cnt.as<int32_t>();
-    rb.needs = s->needs.as<uint8_t>();  // now: 1 = collection overflowed
-    rerank_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(rb);
-    BF_CUDA(cudaGetLastError(), "rerank (pass B)");
   }
+
   // outputs
   int32_t* o_ids = ids;
   float* o_d = dists;
@@ -986,33 +1090,24 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
     o_c = s->h_counts.as<int32_t>();
   }
   finish_kernel<<<(unsigned)((nq + 127) / 128), 128, 0, st>>>(
-      s->out_id.as<int32_t>(), s->out_key.as<DF>(), s->out_cnt.as<int32_t>(), s->fin_id.as<int32_t>(),
-      s->fin_key.as<DF>(), s->fin_cnt.as<int32_t>(), pass_b ? s->qact.as<uint8_t>() : nullptr, (int)nq, k, kmax,
-      space, s->qn_hi.as<float>(), s->qn_lo.as<float>(), h->dev.ext_id, o_ids, o_d, o_c);
+      s->fin_id.as<int32_t>(), s->fin_key.as<DF>(), s->fin_cnt.as<int32_t>(), (int)nq, k, kmax, space,
+      s->qn_hi.as<float>(), s->qn_lo.as<float>(), h->dev.ext_id, o_ids, o_d, o_c);
   BF_CUDA(cudaGetLastError(), "finish");
-  int64_t n_overflow = 0;
-  if (pass_b) {
-    std::vector<uint8_t> ov(nq);
-    BF_CUDA(cudaMemcpyAsync(ov.data(), s->needs.p, nq, cudaMemcpyDeviceToHost, st), "copy flags");
-    BF_CUDA(cudaMemcpyAsync(&dstatus, s->status.p, 4, cudaMemcpyDeviceToHost, st), "copy status");
-    BF_CUDA(cudaStreamSynchronize(st), "brute force pass B");
-    for (int64_t i = 0; i < nq; ++i) n_overflow += ov[i] && needs[i];
-    if (dstatus) return bf_fail(dstatus, "brute-force scan reported a device-side error");
-  }
   if (!dev_ptrs) {
     BF_CUDA(cudaMemcpyAsync(ids, o_ids, (size_t)nq * kmax * 4, cudaMemcpyDeviceToHost, st), "copy ids");
     BF_CUDA(cudaMemcpyAsync(dists, o_d, (size_t)nq * kmax * 4, cudaMemcpyDeviceToHost, st), "copy distances");
     BF_CUDA(cudaMemcpyAsync(counts, o_c, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
-    BF_CUDA(cudaStreamSynchronize(st), "copy results");
   }
+  BF_CUDA(cudaStreamSynchronize(st), "brute-force results");
   if (stats) {
-    stats[0] = nq - n_uncert;  // certified after pass A
-    stats[1] = n_uncert;       // resolved by pass B
-    stats[2] = n_overflow;
+    stats[0] = (int64_t)s_tiles * BN;  // sample rows (the last tile may be partial)
+    stats[1] = max_collected;
+    stats[2] = rescanned;
     stats[3] = n_chunks;
   }
-  if (n_overflow)
-    return bf_fail(NMSG_ERR_CAPACITY, std::to_string(n_overflow) + " queries had more than 16384 vectors within the "
-                                      "BF16 error bound of their k-th neighbour");
+  if (overflow)
+    return bf_fail(NMSG_ERR_CAPACITY, std::to_string(overflow) + " queries had more vectors within the BF16 error "
+                                      "bound of their k-th neighbour than the scan keeps (" + std::to_string(CAND) +
+                                      " per " + std::to_string(chunk_tiles * BN / HALVES) + " base rows)");
   return NMSG_OK;
 }

@@ -57,7 +57,7 @@ def test_bruteforce_matches_fp64(name, k):
     np.testing.assert_array_equal(cnt, np.full(len(q), min(k, n)))
     np.testing.assert_array_equal(ids[:, : min(k, n)], want_i)
     np.testing.assert_allclose(d[:, : min(k, n)], want_d, rtol=2e-6, atol=2e-6)
-    assert st[0] + st[1] == len(q) and st[2] == 0
+    assert st[0] >= 1 and st[1] >= min(k, n) and st[2] == 0
 
 
 def test_bruteforce_limits():
@@ -83,3 +83,42 @@ def test_bruteforce_larger_cosine(tmp_path):
     want_i, want_d = fp64_topk(p, q, 10, "cosinesimil")
     np.testing.assert_array_equal(ids, want_i)
     np.testing.assert_allclose(d, want_d, rtol=2e-6, atol=2e-6)
+
+
+def _far_medium_near(n=40_000, dim=16, seed=5):
+    """A base whose sampled tiles hold only far vectors, so the sample's threshold admits every
+    other vector: more than the collection holds. Tile t (256 rows) is sampled when t % 9 == 0
+    and t <= 135 (16 of the 157 tiles). Ten near vectors sit in tile 1."""
+    rng = np.random.default_rng(seed)
+    u = rng.standard_normal((n, dim))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    tile = np.arange(n) // 256
+    sampled = (tile % 9 == 0) & (tile <= 135)
+    radius = np.where(sampled, 100.0, 10.0 + 5.0 * rng.random(n))
+    radius[256:266] = 1.0 + 0.01 * np.arange(10)
+    return (u * radius[:, None]).astype(np.float32), (0.01 * rng.standard_normal((4, dim))).astype(np.float32)
+
+
+def test_bruteforce_rescans_overflowed_queries(tmp_path):
+    base, q = _far_medium_near()
+    p = str(tmp_path / "fmn.hnsw")
+    _capi.build_index(base, 0, 8, 40, nthreads=0, out_path=p)
+    idx = nmslib.init(method="hnsw", space="l2")
+    idx.loadIndex(p)
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, 10, stats=True)
+    want_i, want_d = fp64_topk(p, q, 10, "l2")
+    np.testing.assert_array_equal(ids, want_i)
+    np.testing.assert_array_equal(np.sort(ids, axis=1), np.tile(np.arange(256, 266), (len(q), 1)))
+    np.testing.assert_allclose(d, want_d, rtol=2e-6, atol=2e-6)
+    assert st[1] > 16384 and st[2] == len(q)
+
+
+def test_bruteforce_capacity_error(tmp_path):
+    """17000 identical vectors: every one stays within the error bound of the k-th, twice."""
+    base = np.tile(np.linspace(-1, 1, 8, dtype=np.float32), (17_000, 1))
+    p = str(tmp_path / "same.hnsw")
+    _capi.build_index(base, 0, 4, 10, nthreads=0, out_path=p)
+    idx = nmslib.init(method="hnsw", space="l2")
+    idx.loadIndex(p)
+    with pytest.raises(RuntimeError, match="within the BF16 error bound"):
+        idx.bruteForceBatchArrays(base[:2] + 0.5, 10)
