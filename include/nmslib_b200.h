@@ -51,8 +51,10 @@ enum nmsg_status {
   NMSG_ERR_CAPACITY = -8       /* a per-query device buffer would overflow */
 };
 
-/* Space names of nmslib.init(space=...): 'l2', 'cosinesimil', 'negdotprod'. */
-enum nmsg_space { NMSG_SPACE_L2 = 0, NMSG_SPACE_COSINE = 1, NMSG_SPACE_NEGDOT = 2 };
+/* Space names of nmslib.init(space=...): 'l2', 'cosinesimil', 'negdotprod', 'l1', 'linf'. The
+ * last two are the optimized index's distance codes 5 and 6 (L1NormSIMD / LInfNormSIMD,
+ * similarity_search/src/method/hnsw.cc:83-89, src/distcomp_lp.cc:77-251). */
+enum nmsg_space { NMSG_SPACE_L2 = 0, NMSG_SPACE_COSINE = 1, NMSG_SPACE_NEGDOT = 2, NMSG_SPACE_L1 = 3, NMSG_SPACE_LINF = 4 };
 
 /* algoType of setQueryTimeParams (hnsw.cc:486-497): hybrid uses SearchOld when ef >= 1000. */
 enum nmsg_algo { NMSG_ALGO_HYBRID = 0, NMSG_ALGO_OLD = 1, NMSG_ALGO_V1MERGE = 2 };
@@ -118,7 +120,8 @@ NMSG_API int nmsg_knn_batch(nmsg_index* index, const float* queries, int64_t nq,
  * maxM = M, maxM0 = 2M, mult = 1/ln M, neighbour heuristic 2. `ids` (optional) are the
  * external ids (addDataPointBatch ids=...), else row numbers. nthreads <= 0: all cores.
  * Node levels are a deterministic function of `seed`; the links depend on thread timing, as in
- * the reference's multi-threaded build. */
+ * the reference's multi-threaded build. Spaces l2, cosinesimil and negdotprod (l1 / linf
+ * indices come from the reference's createIndex: NMSG_ERR_UNSUPPORTED). */
 NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t dim, const int32_t* ids, int space, int M,
                               int ef_construction, int nthreads, uint64_t seed, const char* out_path);
 

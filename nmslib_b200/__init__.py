@@ -3,7 +3,7 @@
 Drop-in for the reference's ``nmslib`` module on this path::
 
     import nmslib_b200 as nmslib
-    index = nmslib.init(method='hnsw', space='l2')        # 'l2' | 'cosinesimil' | 'negdotprod'
+    index = nmslib.init(method='hnsw', space='l2')        # 'l2' | 'cosinesimil' | 'negdotprod' | 'l1' | 'linf'
     index.loadIndex('index.hnsw')                          # a file written by the reference's saveIndex
     index.setQueryTimeParams({'efSearch': 100})
     results = index.knnQueryBatch(queries, k=10)           # [(ids int32[], dists float32[]), ...]
@@ -24,7 +24,8 @@ from . import _capi
 
 __version__ = "0.1.0"
 
-SPACES = {"l2": _capi.SPACE_L2, "cosinesimil": _capi.SPACE_COSINE, "negdotprod": _capi.SPACE_NEGDOT}
+SPACES = {"l2": _capi.SPACE_L2, "cosinesimil": _capi.SPACE_COSINE, "negdotprod": _capi.SPACE_NEGDOT,
+          "l1": _capi.SPACE_L1, "linf": _capi.SPACE_LINF}
 METHODS = ("hnsw",)
 _ALGOS = {"hybrid": _capi.ALGO_HYBRID, "old": _capi.ALGO_OLD, "v1merge": _capi.ALGO_V1MERGE}
 

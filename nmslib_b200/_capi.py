@@ -17,7 +17,7 @@ OK = 0
 ERR_BAD_FILE, ERR_UNSUPPORTED, ERR_BAD_ARG, ERR_OOM = -1, -2, -3, -4
 ERR_DEVICE, ERR_TIMEOUT, ERR_CORRUPT_GRAPH, ERR_CAPACITY = -5, -6, -7, -8
 
-SPACE_L2, SPACE_COSINE, SPACE_NEGDOT = 0, 1, 2
+SPACE_L2, SPACE_COSINE, SPACE_NEGDOT, SPACE_L1, SPACE_LINF = 0, 1, 2, 3, 4
 ALGO_HYBRID, ALGO_OLD, ALGO_V1MERGE = 0, 1, 2
 FLAG_DEVICE_PTRS, FLAG_PLAIN_KERNEL, FLAG_CUDA_GRAPH = 1, 2, 4
 

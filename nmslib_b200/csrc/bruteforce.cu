@@ -873,6 +873,8 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   if (!h) return bf_fail(NMSG_ERR_BAD_ARG, "Must call createIndex or loadIndex before this method");
   if (nq < 0 || k < 1 || kmax < k) return bf_fail(NMSG_ERR_BAD_ARG, "nq must be >= 0, k >= 1 and kmax >= k");
   if (k > CAND) return bf_fail(NMSG_ERR_UNSUPPORTED, "brute force supports k <= 32");
+  if (h->space != NMSG_SPACE_L2 && h->space != NMSG_SPACE_COSINE && h->space != NMSG_SPACE_NEGDOT)
+    return bf_fail(NMSG_ERR_UNSUPPORTED, "brute force on the tensor cores supports l2, cosinesimil and negdotprod");
   if (nq > 0 && (!queries || !ids || !dists || !counts)) return bf_fail(NMSG_ERR_BAD_ARG, "null buffer");
   std::lock_guard<std::mutex> lk(h->mu);
   const bool dev_ptrs = flags & NMSG_DEVICE_PTRS;

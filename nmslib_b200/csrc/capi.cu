@@ -99,6 +99,8 @@ int space_matches(int space, int dist_type) {
     case NMSG_SPACE_L2: return dist_type == kL2Sqr16Ext || dist_type == kL2SqrExt;
     case NMSG_SPACE_COSINE: return dist_type == kNormCosine;
     case NMSG_SPACE_NEGDOT: return dist_type == kNegDot;
+    case NMSG_SPACE_L1: return dist_type == kL1;
+    case NMSG_SPACE_LINF: return dist_type == kLInf;
   }
   return 0;
 }
@@ -119,7 +121,9 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
   // (4.10M q/s at 64 vs 3.47M for two register rows per 8-lane group), 4 rows at efSearch 256
   // (1.90M vs 1.64M), where the larger beam array leaves less shared memory per warp.
   p.stage_rows = 0;
-  if (cfg.stage_rows > 0) {
+  if (d.dist_type == kL1 || d.dist_type == kLInf) {
+    p.gather = kLpGather;  // the only kernels compiled with the L1 / LInf distances
+  } else if (cfg.stage_rows > 0) {
     p.gather = 0;
     p.stage_rows = cfg.stage_rows;
   } else if (cfg.stage_rows == 0 && cfg.rows_per_group == 0 && d.pitch <= 256) {

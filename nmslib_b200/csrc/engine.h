@@ -16,7 +16,10 @@
 namespace nmsg {
 
 // Optimized-index distance codes (similarity_search/include/method/hnsw.h:50-58).
-enum DistCode { kL2Sqr16Ext = 1, kL2SqrExt = 2, kNormCosine = 3, kNegDot = 4 };
+enum DistCode { kL2Sqr16Ext = 1, kL2SqrExt = 2, kNormCosine = 3, kNegDot = 4, kL1 = 5, kLInf = 6 };
+// Gather code of the kernels compiled for L1 / LInf (one row per 8-lane group in registers);
+// 0 = rows staged in shared memory, 1 / 2 / 4 = register rows per group for the other codes.
+constexpr int kLpGather = 3;
 
 // The index as read from an optimized HNSW file, in host memory.
 // File layout (similarity_search/src/method/hnsw.cc:774-806):

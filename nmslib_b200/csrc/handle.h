@@ -23,7 +23,7 @@ constexpr int kMaxSmemPerBlock = 227 * 1024;
 
 // Launch shape of one search launch (see plan_launch).
 struct LaunchPlan {
-  int gather = 1;         // 0: staged rows in shared memory; 1/2/4: register rows per 8-lane group
+  int gather = 1;         // 0: staged rows in shared memory; 1/2/4: register rows per 8-lane group; 3: L1 / LInf
   int stage_rows = 0;
   int hash_log2 = 0;
   int region = 0;         // shared-memory items per warp (beam array or SearchOld heaps)

@@ -259,6 +259,10 @@ using namespace nmsg;
 extern "C" NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t dim, const int32_t* ids,
                                          int space, int M, int ef_construction, int nthreads, uint64_t seed,
                                          const char* out_path) {
+  if (space == NMSG_SPACE_L1 || space == NMSG_SPACE_LINF) {
+    g_build_err = "the host builder supports l2, cosinesimil and negdotprod; build l1 / linf indices with the reference";
+    return NMSG_ERR_UNSUPPORTED;
+  }
   if (!data || n < 0 || dim <= 0 || !out_path || M < 2 || ef_construction < 1 || space < 0 || space > 2) {
     g_build_err = "invalid build arguments";
     return NMSG_ERR_BAD_ARG;

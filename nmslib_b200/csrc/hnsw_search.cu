@@ -93,6 +93,94 @@ __device__ __forceinline__ float combine(const DevIndex& ix, float acc, const fl
   return s;
 }
 
+// L1 (code 5) and LInf (code 6) of one row, by the 8 lanes of a group; every lane of the group
+// returns the value. `row` is in global memory (GLOBAL) or in the warp's staging area.
+//  * L1 restates distcomp_lp.cc:191-251: four float accumulators, accumulator a summing
+//    |q_e - x_e| over e == a (mod 4) in element order with unfused adds, then
+//    ((s0 + s1) + s2) + s3 in float, then the last dim % 4 elements added in double. In the
+//    permuted layout lane j holds e == j (mod 8), so accumulator a (lane a < 4) takes lane a+4's
+//    values by shuffle and interleaves them: a, a+4, a+8, a+12, ...
+//  * LInf (distcomp_lp.cc:77-136) is the maximum of non-negative values: any order gives it.
+template <bool GLOBAL>
+__device__ __forceinline__ float4 ld_row4(const float* p) {
+  if (GLOBAL) return __ldg(reinterpret_cast<const float4*>(p));
+  return *reinterpret_cast<const float4*>(p);
+}
+template <bool GLOBAL>
+__device__ __forceinline__ float2 ld_row2(const float* p) {
+  if (GLOBAL) return __ldg(reinterpret_cast<const float2*>(p));
+  return *reinterpret_cast<const float2*>(p);
+}
+template <bool GLOBAL>
+__device__ __forceinline__ float ld_row1(const float* p) {
+  if (GLOBAL) return __ldg(p);
+  return *p;
+}
+
+template <bool GLOBAL>
+__device__ float lp_group_dist(const DevIndex& ix, const float* __restrict__ q, const float* __restrict__ row,
+                               bool act) {
+  const int lane = lane_id();
+  const int gb = lane & ~7, j = lane & 7;
+  const int nfull = ix.n16 >> 5;
+  const bool half = (ix.n16 & 31) != 0;
+  const bool l1 = ix.dist_type == kL1;
+  float s = 0.0f;  // L1: accumulator j of lanes j < 4; LInf: this lane's maximum
+  for (int c = 0; c < nfull; ++c) {
+    const float4 qv = reinterpret_cast<const float4*>(q + c * 32)[j];
+    const float4 xv = act ? ld_row4<GLOBAL>(row + c * 32 + 4 * j) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 d = make_float4(fabsf(__fsub_rn(qv.x, xv.x)), fabsf(__fsub_rn(qv.y, xv.y)),
+                                 fabsf(__fsub_rn(qv.z, xv.z)), fabsf(__fsub_rn(qv.w, xv.w)));
+    if (l1) {
+      const float4 e = make_float4(__shfl_down_sync(kFull, d.x, 4, 8), __shfl_down_sync(kFull, d.y, 4, 8),
+                                   __shfl_down_sync(kFull, d.z, 4, 8), __shfl_down_sync(kFull, d.w, 4, 8));
+      s = __fadd_rn(s, d.x);
+      s = __fadd_rn(s, e.x);
+      s = __fadd_rn(s, d.y);
+      s = __fadd_rn(s, e.y);
+      s = __fadd_rn(s, d.z);
+      s = __fadd_rn(s, e.z);
+      s = __fadd_rn(s, d.w);
+      s = __fadd_rn(s, e.w);
+    } else {
+      s = fmaxf(fmaxf(fmaxf(s, d.x), fmaxf(d.y, d.z)), d.w);
+    }
+  }
+  if (half) {
+    const float2 qv = reinterpret_cast<const float2*>(q + nfull * 32)[j];
+    const float2 xv = act ? ld_row2<GLOBAL>(row + nfull * 32 + 2 * j) : make_float2(0.f, 0.f);
+    const float2 d = make_float2(fabsf(__fsub_rn(qv.x, xv.x)), fabsf(__fsub_rn(qv.y, xv.y)));
+    if (l1) {
+      const float2 e = make_float2(__shfl_down_sync(kFull, d.x, 4, 8), __shfl_down_sync(kFull, d.y, 4, 8));
+      s = __fadd_rn(s, d.x);
+      s = __fadd_rn(s, e.x);
+      s = __fadd_rn(s, d.y);
+      s = __fadd_rn(s, e.y);
+    } else {
+      s = fmaxf(s, fmaxf(d.x, d.y));
+    }
+  }
+  const int n4 = (ix.dim >> 2) << 2;
+  if (l1) {
+    // [n16, n4): accumulator j continues in natural order
+    if (act && j < 4)
+      for (int e = ix.n16 + j; e < n4; e += 4) s = __fadd_rn(s, fabsf(__fsub_rn(q[e], ld_row1<GLOBAL>(row + e))));
+    float t = __fadd_rn(__shfl_sync(kFull, s, gb), __shfl_sync(kFull, s, gb + 1));
+    t = __fadd_rn(t, __shfl_sync(kFull, s, gb + 2));
+    t = __fadd_rn(t, __shfl_sync(kFull, s, gb + 3));
+    double r = (double)t;
+    if (act)
+      for (int e = n4; e < ix.dim; ++e) r = __dadd_rn(r, (double)fabsf(__fsub_rn(q[e], ld_row1<GLOBAL>(row + e))));
+    return __double2float_rn(r);
+  }
+  if (act)
+    for (int e = ix.n16 + j; e < ix.dim; e += 8) s = fmaxf(s, fabsf(__fsub_rn(q[e], ld_row1<GLOBAL>(row + e))));
+  s = fmaxf(s, __shfl_xor_sync(kFull, s, 4, 8));
+  s = fmaxf(s, __shfl_xor_sync(kFull, s, 2, 8));
+  s = fmaxf(s, __shfl_xor_sync(kFull, s, 1, 8));
+  return s;
+}
+
 // Distances from the query (shared memory, permuted) to rows ids[0..n), written to out[0..n).
 // Four 8-lane groups per warp, R rows per group in flight.
 template <int R>
@@ -103,49 +191,60 @@ __device__ void compute_dists(const DevIndex& ix, const float* __restrict__ q, c
   const int nfull = ix.n16 >> 5;
   const bool half = (ix.n16 & 31) != 0;
   const int code = ix.dist_type;
-  for (int base = 0; base < n; base += 4 * R) {
-    const float* rows[R];
-    bool act[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int idx = base + g + 4 * r;
-      act[r] = idx < n;
-      rows[r] = ix.vecs + (int64_t)(act[r] ? ids[idx] : 0) * ix.pitch;
+  if constexpr (R == kLpGather) {  // L1 / LInf indices run kernels of their own (gather code 3)
+    for (int base = 0; base < n; base += 4) {
+      const int idx = base + g;
+      const bool act = idx < n;
+      const float* row = ix.vecs + (int64_t)(act ? ids[idx] : 0) * ix.pitch;
+      const float d = lp_group_dist<true>(ix, q, row, act);
+      if (act && j == 0) out[idx] = d;
     }
-    float acc[R];
+    __syncwarp();
+  } else {
+    for (int base = 0; base < n; base += 4 * R) {
+      const float* rows[R];
+      bool act[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) acc[r] = 0.0f;
+      for (int r = 0; r < R; ++r) {
+        const int idx = base + g + 4 * r;
+        act[r] = idx < n;
+        rows[r] = ix.vecs + (int64_t)(act[r] ? ids[idx] : 0) * ix.pitch;
+      }
+      float acc[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[r] = 0.0f;
 #pragma unroll 4
-    for (int c = 0; c < nfull; ++c) {
-      const float4 qv = reinterpret_cast<const float4*>(q + c * 32)[j];
-      float4 x[R];
+      for (int c = 0; c < nfull; ++c) {
+        const float4 qv = reinterpret_cast<const float4*>(q + c * 32)[j];
+        float4 x[R];
 #pragma unroll
-      for (int r = 0; r < R; ++r)
-        x[r] = act[r] ? __ldg(reinterpret_cast<const float4*>(rows[r] + c * 32) + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int r = 0; r < R; ++r)
+          x[r] = act[r] ? __ldg(reinterpret_cast<const float4*>(rows[r] + c * 32) + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          acc[r] = fma_term(code, qv.x, x[r].x, acc[r]);
+          acc[r] = fma_term(code, qv.y, x[r].y, acc[r]);
+          acc[r] = fma_term(code, qv.z, x[r].z, acc[r]);
+          acc[r] = fma_term(code, qv.w, x[r].w, acc[r]);
+        }
+      }
+      if (half) {
+        const float2 qv = reinterpret_cast<const float2*>(q + nfull * 32)[j];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const float2 x = act[r] ? __ldg(reinterpret_cast<const float2*>(rows[r] + nfull * 32) + j) : make_float2(0.f, 0.f);
+          acc[r] = fma_term(code, qv.x, x.x, acc[r]);
+          acc[r] = fma_term(code, qv.y, x.y, acc[r]);
+        }
+      }
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        acc[r] = fma_term(code, qv.x, x[r].x, acc[r]);
-        acc[r] = fma_term(code, qv.y, x[r].y, acc[r]);
-        acc[r] = fma_term(code, qv.z, x[r].z, acc[r]);
-        acc[r] = fma_term(code, qv.w, x[r].w, acc[r]);
+        const float d = combine(ix, acc[r], rows[r], q);
+        if (act[r] && j == 0) out[base + g + 4 * r] = d;
       }
     }
-    if (half) {
-      const float2 qv = reinterpret_cast<const float2*>(q + nfull * 32)[j];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const float2 x = act[r] ? __ldg(reinterpret_cast<const float2*>(rows[r] + nfull * 32) + j) : make_float2(0.f, 0.f);
-        acc[r] = fma_term(code, qv.x, x.x, acc[r]);
-        acc[r] = fma_term(code, qv.y, x.y, acc[r]);
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const float d = combine(ix, acc[r], rows[r], q);
-      if (act[r] && j == 0) out[base + g + 4 * r] = d;
-    }
+    __syncwarp();
   }
-  __syncwarp();
 }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -770,7 +869,7 @@ __device__ void greedy_descent(const SearchArgs& a, WarpCtx& w, int& cur_out, fl
   int cur = ix.enterpoint;
   if (lane == 0) w.nb_id[0] = cur;
   __syncwarp();
-  compute_dists<1>(ix, w.q, w.nb_id, 1, w.nb_d);
+  compute_dists<(R == kLpGather ? kLpGather : 1)>(ix, w.q, w.nb_id, 1, w.nb_d);
   float curdist = w.nb_d[0];
   w.st_dist += 1;
   w.st_bytes += 4LL * ix.dim;
@@ -1125,6 +1224,7 @@ Kern pick(bool plain, int gather) {
       case 0: return search_plain_kernel<0, OLD>;
       case 1: return search_plain_kernel<1, OLD>;
       case 2: return search_plain_kernel<2, OLD>;
+      case kLpGather: return search_plain_kernel<kLpGather, OLD>;
       default: return search_plain_kernel<4, OLD>;
     }
   }
@@ -1132,6 +1232,7 @@ Kern pick(bool plain, int gather) {
     case 0: return search_batched_kernel<0, OLD>;
     case 1: return search_batched_kernel<1, OLD>;
     case 2: return search_batched_kernel<2, OLD>;
+    case kLpGather: return search_batched_kernel<kLpGather, OLD>;
     default: return search_batched_kernel<4, OLD>;
   }
 }

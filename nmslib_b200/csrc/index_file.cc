@@ -116,11 +116,7 @@ int read_index_file(const char* path, HostIndex& ix, std::string& err) {
 
 int validate_index(const HostIndex& ix, std::string& err) {
   if (ix.empty_regular) return NMSG_OK;
-  if (ix.dist_type == 5 || ix.dist_type == 6) {
-    err = "L1/LInf optimized indices are not supported by the B200 engine";
-    return NMSG_ERR_UNSUPPORTED;
-  }
-  if (ix.dist_type < 1 || ix.dist_type > 4) {
+  if (ix.dist_type < 1 || ix.dist_type > 6) {
     err = "Unknown distance function code: " + std::to_string(ix.dist_type);
     return NMSG_ERR_BAD_FILE;
   }

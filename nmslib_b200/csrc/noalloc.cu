@@ -119,7 +119,7 @@ extern "C" NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* h, const float* queri
   a.region_items = ((old ? ef + 1 + k : std::max(ef, k)) + 1) & ~1;
   a.hash_log2 = 0;
   a.stage_rows = 0;
-  const int gather = d.pitch <= 256 ? 2 : 1;
+  const int gather = (d.dist_type == kL1 || d.dist_type == kLInf) ? kLpGather : (d.pitch <= 256 ? 2 : 1);
   a.warp_smem = warp_smem_bytes(d, a.region_items, a.nbpad, 0, 0);
   int wpb = 4;
   while (wpb > 1 && wpb * a.warp_smem > kNoAllocMaxSmemPerBlock) wpb >>= 1;

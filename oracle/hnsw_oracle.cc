@@ -8,7 +8,8 @@
 //                                 and the writer it mirrors, hnsw.cc:774-806
 //   * distance kernels          — similarity_search/include/method/hnsw_distfunc_opt_impl_inline.h:42-173
 //                                 (AVX L2Sqr16Ext / L2SqrExt / ScalarProduct, FMA-contracted lane order)
-//                                 and the wrappers at src/method/hnsw.cc:70-102
+//                                 and the wrappers at src/method/hnsw.cc:70-102; L1 / LInf
+//                                 (dist codes 5 / 6) from similarity_search/src/distcomp_lp.cc:77-251
 //   * query normalisation       — similarity_search/include/method/hnsw.h:486-497 (NormalizeVect)
 //   * greedy upper-level descent — src/method/hnsw_distfunc_opt.cc:62-92 and :168-198
 //   * level-0 beam, V1Merge     — src/method/hnsw_distfunc_opt.cc:200-283 with the sorted-array
@@ -37,7 +38,7 @@
 
 namespace {
 
-enum DistType { kL2Sqr16Ext = 1, kL2SqrExt = 2, kNormCosine = 3, kNegDot = 4 };
+enum DistType { kL2Sqr16Ext = 1, kL2SqrExt = 2, kNormCosine = 3, kNegDot = 4, kL1 = 5, kLInf = 6 };
 
 struct OracleIndex {
   uint32_t n = 0;
@@ -117,6 +118,26 @@ float dot_avx(const float* a, const float* b, int dim) {
   return s;
 }
 
+// distcomp_lp.cc:191-251 (L1NormSIMD, SSE path): 4 float lanes over the first dim/4*4
+// elements, lane j summing |a_e - b_e| for e == j (mod 4) in element order, unfused adds; the
+// lanes are summed left to right in float, and the remaining elements are added in double.
+float l1_sse(const float* a, const float* b, int dim) {
+  float acc[4] = {0, 0, 0, 0};
+  const int n4 = (dim >> 2) << 2;
+  for (int e = 0; e < n4; ++e) acc[e & 3] = acc[e & 3] + std::fabs(a[e] - b[e]);
+  double res = ((acc[0] + acc[1]) + acc[2]) + acc[3];
+  for (int e = n4; e < dim; ++e) res += std::fabs(a[e] - b[e]);
+  return (float)res;
+}
+
+// distcomp_lp.cc:77-136 (LInfNormSIMD): the largest |a_e - b_e|; a maximum of non-negative
+// values, so the lane structure does not change the result.
+float linf_sse(const float* a, const float* b, int dim) {
+  float res = 0.0f;
+  for (int e = 0; e < dim; ++e) res = std::max(res, std::fabs(a[e] - b[e]));
+  return res;
+}
+
 float dist(int type, const float* q, const float* v, int dim) {
   switch (type) {
     case kL2Sqr16Ext: return l2sqr16(q, v, dim);
@@ -126,6 +147,8 @@ float dist(int type, const float* q, const float* v, int dim) {
       return std::max(0.0f, 1 - std::max(-1.0f, std::min(1.0f, d)));
     }
     case kNegDot: return -dot_avx(q, v, dim);  // hnsw.cc:70-73
+    case kL1: return l1_sse(q, v, dim);          // hnsw.cc:83-85
+    case kLInf: return linf_sse(q, v, dim);      // hnsw.cc:87-89
   }
   return NAN;
 }

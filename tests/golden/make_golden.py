@@ -3,7 +3,7 @@
 Run once, where the reference sources are available:
 
     make -C oracle ref          # builds oracle/_ref/nmslib*.so from the reference sources
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]   # all cases, or only the named ones
 
 For every case it builds an HNSW index with the reference's own ``createIndex`` (single
 index thread, so the build is reproducible), writes the reference's ``saveIndex`` file as
@@ -58,15 +58,32 @@ def cases():
     base = np.repeat(x[:100], 3, axis=0)
     c["dup_l2_d16"] = ("l2", base, x[100:], 6, 60, [(10, 24, "hybrid"), (10, 24, "old"), (30, 200, "hybrid")],
                        None)
+    # L1 / LInf (dist codes 5 / 6): dim 22 has a final 16-block, a 4-wide remainder and a
+    # 2-element tail that L1 sums in double; dim 64 is whole 32-chunks; dim 37 has every part
+    x = mixture("gauss", 1_050, 22, 20, 21, 0.4)
+    c["l1_d22"] = ("l1", x[:1_000], x[1_000:], 8, 60, [(10, 40, "hybrid"), (10, 1000, "hybrid"), (5, 30, "old")],
+                   None)
+    x = mixture("gauss", 1_550, 64, 30, 22, 0.3)
+    c["l1_d64"] = ("l1", x[:1_500], x[1_500:], 12, 100, [(10, 64, "hybrid"), (20, 200, "v1merge")], None)
+    x = mixture("gauss", 1_050, 37, 20, 23, 0.4)
+    c["linf_d37"] = ("linf", x[:1_000], x[1_000:], 8, 60, [(10, 50, "hybrid"), (10, 1000, "hybrid")], None)
+    x = mixture("gauss", 1_550, 128, 30, 24, 0.3)
+    c["linf_d128"] = ("linf", x[:1_500], x[1_500:], 12, 100, [(10, 64, "hybrid"), (1, 16, "hybrid")], None)
     return c
 
 
-def main():
+def main(only=None):
     ref = reference_module()
     if ref is None:
         raise SystemExit("reference module not built: run `make -C oracle ref` first")
     manifest = {}
+    mpath = os.path.join(HERE, "manifest.json")
+    if only and os.path.exists(mpath):  # regenerate only the named cases, keep the others
+        with open(mpath) as f:
+            manifest = json.load(f)
     for name, (space, base, queries, m, efc, settings, ids) in cases().items():
+        if only and name not in only:
+            continue
         index = ref.init(method="hnsw", space=space)
         if ids is None:
             index.addDataPointBatch(base)
@@ -94,9 +111,9 @@ def main():
                           "settings": [list(s) for s in settings], "n": int(len(base)),
                           "dim": int(base.shape[1]), "nq": int(len(queries))}
         print(name, os.path.getsize(path), "bytes")
-    with open(os.path.join(HERE, "manifest.json"), "w") as f:
+    with open(mpath, "w") as f:
         json.dump(manifest, f, indent=1)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

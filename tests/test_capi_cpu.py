@@ -88,7 +88,10 @@ def test_unsupported_files(lib, tmp_path):
     struct.pack_into("<i", bad, 4 + 4 + 8 * 3 + 4 + 4 + 8 + 8, 5)  # dist_func_type := L1
     p = tmp_path / "l1.hnsw"
     p.write_bytes(bytes(bad))
-    assert _load_rc(lib, str(p))[0] == _capi.ERR_UNSUPPORTED
+    assert _load_rc(lib, str(p))[0] == _capi.ERR_BAD_ARG  # an L1 index opened as l2
+    struct.pack_into("<i", bad, 4 + 4 + 8 * 3 + 4 + 4 + 8 + 8, 9)  # no such distance code
+    p.write_bytes(bytes(bad))
+    assert _load_rc(lib, str(p))[0] == _capi.ERR_BAD_FILE
     p.write_bytes(struct.pack("<II", 0, 10) + b"\0" * 64)  # regular format with elements
     assert _load_rc(lib, str(p))[0] == _capi.ERR_UNSUPPORTED
     # wrong space for the file
@@ -99,7 +102,9 @@ def test_python_surface_errors():
     with pytest.raises(ValueError):
         nmslib.init(method="sw-graph", space="l2")
     with pytest.raises(ValueError):
-        nmslib.init(method="hnsw", space="l1")
+        nmslib.init(method="hnsw", space="l3")
+    nmslib.init(method="hnsw", space="l1")  # the optimized index's L1 / LInf codes are served
+    nmslib.init(method="hnsw", space="linf")
     idx = nmslib.init(method="hnsw", space="l2")
     with pytest.raises(ValueError, match="Must call createIndex or loadIndex"):
         idx.knnQueryBatch(np.zeros((2, 4), np.float32))
