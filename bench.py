@@ -241,12 +241,15 @@ def cpu_reference_qps(path, queries, ef, k, target_seconds=3.0, space="l2"):
 
 
 # ------------------------------------------------------------------ serving and brute force
-def serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6), seconds=1.0, seed=11):
+def serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6), seconds=1.0, seed=11, workload=WORKLOAD):
     """p50/p99 request latency and achieved QPS of the continuous-batching server at several
-    offered loads (queries per second), open-loop Poisson arrivals."""
+    offered loads (queries per second), open-loop Poisson arrivals. The memory budget holds 32
+    lanes of 256 query slots (one visited byte per base vector each)."""
     from nmslib_b200.serving import Server
     rng = np.random.default_rng(seed)
-    srv = Server(index, memory_budget_bytes=8 << 30, max_batch=256, max_k=100, max_lanes=32)
+    n = index.info["n"]
+    budget = max(8 << 30, int(32 * 256 * ((n + 15) // 16 * 16 + 1) * 1.05))
+    srv = Server(index, memory_budget_bytes=budget, max_batch=256, max_k=100, max_lanes=32)
     out = []
     try:
         for qps in rates_qps:
@@ -265,7 +268,8 @@ def serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6), seconds=1.0, seed
             log(f"[bench] serving {qps:.0f} q/s offered: {out[-1]}")
     finally:
         srv.close()
-    return {"workload": WORKLOAD + " index, request mix of the 5M serving config", "points": out}
+    return {"workload": workload + " index, request mix of the 5M serving config", "points": out,
+            "memory_budget_bytes": budget}
 
 
 def brute_force_measure(index, queries, k=10, reps=3):
@@ -368,7 +372,7 @@ def run_aux(args):
     if args.workload == "c3":
         out["bruteforce"] = brute_force_measure(index, queries[:10_000])
     if args.workload == "c5":
-        out["serving"] = serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6, 2e6))
+        out["serving"] = serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6, 2e6), workload=name)
     if args.workload == "c4":
         rng = np.random.default_rng(4)
         nq = len(queries)

@@ -164,7 +164,7 @@ NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* index, const float* queries, int
  * reaches; a second BF16 GEMM over the whole base collects the vectors at or above it and the
  * exact rerank orders them. The ids are the exact top-k (ties by id); distances follow the
  * index's space as the HNSW path reports them (squared L2, 1 - cos on normalised vectors, -dot).
- * dim <= 256, k <= 32. The full scan keeps up to 32 vectors per query and per half of a base
+ * dim <= 256, k <= 32. The full scan keeps up to 64 vectors per query and per half of a base
  * chunk; a query that finds more in some chunk is scanned again with a raised threshold (up to
  * three times), and if it still overflows the call returns NMSG_ERR_CAPACITY (many vectors tied
  * with the k-th neighbour within the BF16 error bound). stats (optional, 4 values): sample rows

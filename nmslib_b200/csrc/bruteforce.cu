@@ -52,6 +52,7 @@ constexpr int EPI_WARPS = 8;            // two warps per TMEM lane quarter, one 
 constexpr int HALVES = 2;
 constexpr int kThreads = (EPI_WARPS + 2) * 32;  // + TMA warp + MMA warp
 constexpr int LIST_STRIDE = CAND + 1;   // +1: rows of a list on different banks
+constexpr int kCollectLen = 64;         // entries of a full-scan list (query, chunk, column half)
 
 struct GemmArgs {
   int kb;             // padded dim / 64
@@ -67,10 +68,11 @@ struct GemmArgs {
   int per_column;     // mode 0: offer every column, not only each 32-column group's best
   int key_l2;         // 1: key = 2 dot - |x|^2, 0: key = dot
   const float* xnorm2;  // |x|^2 (l2) or 0, +inf for the padding rows up to n_tiles * BN
-  // one list of CAND entries per (query, chunk, column half), written only by the thread that
-  // owns that query row in that work item: mode 0 the best group maxima, mode 1 the rows whose
-  // key reaches tau (the count may exceed CAND: the list overflowed)
-  float* list_key;    // [nq][n_chunks * HALVES][CAND]
+  // one list of list_len entries per (query, chunk, column half), written only by the thread
+  // that owns that query row in that work item: mode 0 the best group maxima (list_len = CAND),
+  // mode 1 the rows whose key reaches tau (the count may exceed list_len: the list overflowed)
+  int list_len;
+  float* list_key;    // [nq][n_chunks * HALVES][list_len]
   int32_t* list_id;
   int32_t* list_cnt;  // [nq][n_chunks * HALVES]
   const float* tau;   // [nq]
@@ -293,8 +295,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (t0 < t1) nrm_next = __ldg(xn4 + (size_t)t0 * a.tile_step * (BN / 4));
       const float ks = a.key_l2 ? 2.0f : 1.0f;
       const size_t list = ((size_t)q * a.n_chunks + chunk) * HALVES + half;
-      int32_t* cid = a.list_id + list * CAND;
-      float* ckey = a.list_key + list * CAND;
+      int32_t* cid = a.list_id + list * a.list_len;
+      float* ckey = a.list_key + list * a.list_len;
       int ncoll = 0;
       for (int vt = t0; vt < t1 && ok; ++vt, ++tcount) {
         const int t = vt * a.tile_step;
@@ -369,7 +371,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int i = 0; i < 32; ++i)
               if (v[i] >= thr) {
-                if (ncoll < CAND) {
+                if (ncoll < a.list_len) {
                   cid[ncoll] = col0 + i;
                   ckey[ncoll] = v[i];
                 }
@@ -427,10 +429,10 @@ struct RerankArgs {
   const float* xn_hi;    // l2: |x|^2 as double-float
   const float* xn_lo;
   int dim, n, nq, k, l2;
-  int n_lists;                 // lists of CAND entries per query
-  int32_t* ids;                // [nq][n_lists][CAND] internal ids, compacted in place here
+  int n_lists, list_len;       // lists of list_len entries per query
+  int32_t* ids;                // [nq][n_lists][list_len] internal ids, compacted in place here
   float* bf_keys;              // BF16 keys, same layout
-  const int32_t* list_count;   // [nq][n_lists] entries found per list (more than CAND: overflow)
+  const int32_t* list_count;   // [nq][n_lists] entries found per list (more than list_len: overflow)
   const float* eps;            // [nq] bound on |BF16 key - exact key|
   const uint8_t* only;         // optional: rerank only the queries flagged here
   // outputs
@@ -470,12 +472,12 @@ __global__ void rerank_kernel(RerankArgs a) {
   const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (q >= a.nq) return;
   if (a.only && !a.only[q]) return;
-  const size_t base = (size_t)q * a.n_lists * CAND;
+  const size_t base = (size_t)q * a.n_lists * a.list_len;
   int32_t* ids = a.ids + base;
   float* bk = a.bf_keys + base;
   const float eps = a.eps[q];
 
-  // 0. compact the lists in place: list l's first min(count, CAND) entries move to the running
+  // 0. compact the lists in place: list l's first min(count, list_len) entries move to the running
   //    total (never past their own position, and each lane reads before any lane writes)
   int total = 0, found_all = 0;
   bool overflow = false;
@@ -483,26 +485,29 @@ __global__ void rerank_kernel(RerankArgs a) {
   for (int l0 = 0; l0 < a.n_lists; l0 += 32) {
     const int my_cnt = l0 + lane < a.n_lists ? lc[l0 + lane] : 0;
     found_all += my_cnt;
-    overflow |= my_cnt > CAND;
+    overflow |= my_cnt > a.list_len;
     unsigned nonempty = __ballot_sync(0xffffffffu, my_cnt > 0);
     while (nonempty) {
       const int j = __ffs(nonempty) - 1;
       nonempty &= nonempty - 1;
-      const int cnt = min(__shfl_sync(0xffffffffu, my_cnt, j), CAND);
-      const int src = (l0 + j) * CAND + lane;
-      int32_t id = 0;
-      float key = 0.0f;
-      if (lane < cnt) {
-        id = ids[src];
-        key = bk[src];
+      const int cnt = min(__shfl_sync(0xffffffffu, my_cnt, j), a.list_len);
+      for (int c0 = 0; c0 < cnt; c0 += 32) {
+        const int take = min(32, cnt - c0);
+        const int src = (l0 + j) * a.list_len + c0 + lane;
+        int32_t id = 0;
+        float key = 0.0f;
+        if (lane < take) {
+          id = ids[src];
+          key = bk[src];
+        }
+        __syncwarp();
+        if (lane < take) {
+          ids[total + lane] = id;
+          bk[total + lane] = key;
+        }
+        __syncwarp();
+        total += take;
       }
-      __syncwarp();
-      if (lane < cnt) {
-        ids[total + lane] = id;
-        bk[total + lane] = key;
-      }
-      __syncwarp();
-      total += cnt;
     }
   }
 #pragma unroll
@@ -961,8 +966,8 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   BF_CUDA(s->fin_id.ensure((size_t)nq * k * 4, false), "cudaMalloc");
   BF_CUDA(s->fin_key.ensure((size_t)nq * k * 8, false), "cudaMalloc");
   BF_CUDA(s->fin_cnt.ensure(nq * 4, false), "cudaMalloc");
-  BF_CUDA(s->coll_id.ensure(c_lists * CAND * 4, false), "cudaMalloc(collection)");
-  BF_CUDA(s->coll_key.ensure(c_lists * CAND * 4, false), "cudaMalloc(collection)");
+  BF_CUDA(s->coll_id.ensure(c_lists * kCollectLen * 4, false), "cudaMalloc(collection)");
+  BF_CUDA(s->coll_key.ensure(c_lists * kCollectLen * 4, false), "cudaMalloc(collection)");
   BF_CUDA(s->coll_cnt.ensure(c_lists * 4, false), "cudaMalloc(collection)");
   BF_CUDA(s->found.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->status.ensure(4, true), "cudaMalloc");
@@ -992,6 +997,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ga.per_column = s_tiles == n_tiles;
   ga.key_l2 = l2;
   ga.xnorm2 = s->xn.as<float>();
+  ga.list_len = CAND;
   ga.list_key = s->cand_key.as<float>();
   ga.list_id = s->cand_id.as<int32_t>();
   ga.list_cnt = s->cand_cnt.as<int32_t>();
@@ -1015,6 +1021,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ra.k = k;
   ra.l2 = l2;
   ra.n_lists = s_chunks * HALVES;
+  ra.list_len = CAND;
   ra.ids = s->cand_id.as<int32_t>();
   ra.bf_keys = s->cand_key.as<float>();
   ra.list_count = s->cand_cnt.as<int32_t>();
@@ -1037,11 +1044,13 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   gb.tile_step = 1;
   gb.chunk_tiles = chunk_tiles;
   gb.n_chunks = n_chunks;
+  gb.list_len = kCollectLen;
   gb.list_key = s->coll_key.as<float>();
   gb.list_id = s->coll_id.as<int32_t>();
   gb.list_cnt = s->coll_cnt.as<int32_t>();
   RerankArgs rb = ra;
   rb.n_lists = n_chunks * HALVES;
+  rb.list_len = kCollectLen;
   rb.ids = s->coll_id.as<int32_t>();
   rb.bf_keys = s->coll_key.as<float>();
   rb.list_count = s->coll_cnt.as<int32_t>();
@@ -1109,7 +1118,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   }
   if (overflow)
     return bf_fail(NMSG_ERR_CAPACITY, std::to_string(overflow) + " queries had more vectors within the BF16 error "
-                                      "bound of their k-th neighbour than the scan keeps (" + std::to_string(CAND) +
+                                      "bound of their k-th neighbour than the scan keeps (" + std::to_string(kCollectLen) +
                                       " per " + std::to_string(chunk_tiles * BN / HALVES) + " base rows)");
   return NMSG_OK;
 }

@@ -170,7 +170,7 @@ extern "C" {
 int nmsg_index_load(const char* path, int space, int device, nmsg_index** out) {
   if (!out || !path) return fail(NMSG_ERR_BAD_ARG, "null argument");
   *out = nullptr;
-  if (space < 0 || space > 2) return fail(NMSG_ERR_BAD_ARG, "unknown space code");
+  if (space < NMSG_SPACE_L2 || space > NMSG_SPACE_LINF) return fail(NMSG_ERR_BAD_ARG, "unknown space code");
   auto* h = new nmsg_index();
   h->device = device;
   h->space = space;

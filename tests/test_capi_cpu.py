@@ -42,8 +42,11 @@ def _header(path):
     return raw
 
 
-def test_valid_file_reaches_device_check(lib):
-    rc, msg = _load_rc(lib, golden_path("c1_l2_d128"))
+@pytest.mark.parametrize("name,space", [("c1_l2_d128", _capi.SPACE_L2), ("cos_d100", _capi.SPACE_COSINE),
+                                        ("negdot_d960", _capi.SPACE_NEGDOT), ("l1_d22", _capi.SPACE_L1),
+                                        ("linf_d37", _capi.SPACE_LINF)])
+def test_valid_file_reaches_device_check(lib, name, space):
+    rc, msg = _load_rc(lib, golden_path(name), space=space)
     # no GPU in this container: the file passes validation and the device check answers
     import torch
     if torch.cuda.is_available():
