@@ -422,6 +422,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile-case", type=int, default=0, metavar="NQ",
                     help="profiling run: only NQ queries at the headline efSearch, no sweep, no baselines")
+    ap.add_argument("--profile-bruteforce", type=int, default=0, metavar="NQ",
+                    help="profiling run: exact brute force (k=10) of NQ queries over the base, warmup + steps calls")
     ap.add_argument("--workload", choices=["c2", "c3", "c4", "c5"], default="c2",
                     help="c2 (default, the headline line); c3 cosine 1M x 100 + brute force; c4 negdot "
                          "1M x 960 mixed k/ef batch; c5 l2 5M x 96 serving")
@@ -487,6 +489,15 @@ def main():
         end.record(stream)
         torch.cuda.synchronize()
         return start.elapsed_time(end) / steps
+
+    if args.profile_bruteforce:
+        # the tensor-core brute force alone, through the public API, for ncu
+        qs = queries[:args.profile_bruteforce]
+        for _ in range(args.warmup + args.steps):
+            index.bruteForceBatchArrays(qs, K)
+        torch.cuda.synchronize()
+        log(f"[bench] brute-force profile case: {args.warmup + args.steps} calls of {len(qs)} queries")
+        return
 
     if args.profile_case:
         # a small launch of the same kernel for ncu: the full index, a slice of the queries

@@ -64,8 +64,7 @@ struct GemmArgs {
   int chunk_tiles;    // visited tiles per work item
   int n_chunks;
   int q_blocks;
-  int mode;           // 0: top-CAND per (chunk, column half); 1: collect keys >= tau
-  int per_column;     // mode 0: offer every column, not only each 32-column group's best
+  int per_column;     // sample pass: offer every column, not only each 32-column group's best
   int key_l2;         // 1: key = 2 dot - |x|^2, 0: key = dot
   const float* xnorm2;  // |x|^2 (l2) or 0, +inf for the padding rows up to n_tiles * BN
   // one list of list_len entries per (query, chunk, column half), written only by the thread
@@ -94,8 +93,9 @@ struct SmemLayout {
   }
 };
 
+template <int MODE>
 __device__ __forceinline__ bool item_active(const GemmArgs& a, int qb) {
-  if (a.mode == 0) return true;
+  if (MODE == 0) return true;
   const uint8_t* p = a.q_active + (size_t)qb * BM;
   for (int i = 0; i < BM; ++i)
     if (p[i]) return true;
@@ -103,8 +103,9 @@ __device__ __forceinline__ bool item_active(const GemmArgs& a, int qb) {
 }
 
 // First active work item at or after `item` in this CTA's round-robin sequence (n_items if none).
+template <int MODE>
 __device__ __forceinline__ int next_active_item(const GemmArgs& a, int item, int n_items) {
-  while (item < n_items && !item_active(a, item % a.q_blocks)) item += gridDim.x;
+  while (item < n_items && !item_active<MODE>(a, item % a.q_blocks)) item += gridDim.x;
   return item;
 }
 
@@ -144,6 +145,9 @@ __device__ __forceinline__ void list_offer(float* lk, int32_t* li, int& nfill, f
   thr = lk[0];
 }
 
+// MODE 0: the sample pass (per-row candidate heaps); MODE 1: the full scan (threshold lists).
+// Compiled separately so that each carries only its own epilogue code.
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
     bf16_scan_kernel(const __grid_constant__ CUtensorMap tmq, const __grid_constant__ CUtensorMap tmx, GemmArgs a) {
   extern __shared__ uint8_t smem_raw[];
@@ -196,8 +200,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       // items are chunk-major: the CTAs running at the same time read the same base chunk, which
       // stays in L2 while every query block passes over it. The query block is loaded only when
       // it differs from the previous item's (for batches of <= 128 queries, once per CTA).
-      for (int item = next_active_item(a, blockIdx.x, n_items); item < n_items && ok;
-           item = next_active_item(a, item + gridDim.x, n_items)) {
+      for (int item = next_active_item<MODE>(a, blockIdx.x, n_items); item < n_items && ok;
+           item = next_active_item<MODE>(a, item + gridDim.x, n_items)) {
         const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
         if (qb != prev_qb) {
           if (prev_qb >= 0) {
@@ -233,8 +237,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t xphase = 0, qphase = 0;
       uint32_t accphase[2] = {0, 0};
       int tcount = 0, prev_qb = -1;
-      for (int item = next_active_item(a, blockIdx.x, n_items); item < n_items && ok;) {
-        const int next = next_active_item(a, item + gridDim.x, n_items);
+      for (int item = next_active_item<MODE>(a, blockIdx.x, n_items); item < n_items && ok;) {
+        const int next = next_active_item<MODE>(a, item + gridDim.x, n_items);
         const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
         if (qb != prev_qb) {
           ok = mbar_wait(q_full, qphase);
@@ -281,13 +285,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     int tcount = 0;
     for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
       const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
-      if (!item_active(a, qb)) continue;
+      if (!item_active<MODE>(a, qb)) continue;
       const int q = qb * BM + row;
       const bool qvalid = q < a.nq;
       float thr = -INFINITY;  // mode 0: the list's smallest key once full; mode 1: tau
       int nfill = 0;
       // mode 1: a finite floor, so the -inf keys of columns past the last row never qualify
-      if (a.mode == 1) thr = (qvalid && a.q_active[q]) ? fmaxf(a.tau[q], -FLT_MAX) : INFINITY;
+      if (MODE == 1) thr = (qvalid && a.q_active[q]) ? fmaxf(a.tau[q], -FLT_MAX) : INFINITY;
       const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
       // |x|^2 of this half's 128 columns, 4 per lane, loaded one tile ahead
       const float4* xn4 = reinterpret_cast<const float4*>(a.xnorm2) + half * (BN / HALVES / 4) + lane;
@@ -347,43 +351,50 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int i = 0; i < w; ++i) m[i] = fmaxf(m[i], m[i + w]);
           const float mx = m[0];
-          if (a.mode == 0 && a.per_column) {
-            // small bases (the sample is all of it): every column is offered
-            if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
-              float vl[32];
+          if constexpr (MODE == 0) {
+            if (a.per_column) {
+              // small bases (the sample is all of it): every column is offered
+              if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
+                float vl[32];
 #pragma unroll
-              for (int i = 0; i < 32; ++i) vl[i] = v[i];
+                for (int i = 0; i < 32; ++i) vl[i] = v[i];
 #pragma unroll 1
-              for (int i = 0; i < 32; ++i)
-                if ((vl[i] > thr || nfill < CAND) && vl[i] > -INFINITY) list_offer(lk, li, nfill, thr, vl[i], col0 + i);
-            }
-          } else if (a.mode == 0) {
-            // the group's best column is the candidate: the lists hold distinct base vectors,
-            // so the exact k-th key among them still bounds the true k-th key from below
-            if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
+                for (int i = 0; i < 32; ++i)
+                  if ((vl[i] > thr || nfill < CAND) && vl[i] > -INFINITY)
+                    list_offer(lk, li, nfill, thr, vl[i], col0 + i);
+              }
+            } else if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
+              // the group's best column is the candidate: the lists hold distinct base vectors,
+              // so the exact k-th key among them still bounds the true k-th key from below
               int arg = 31;
 #pragma unroll
               for (int i = 30; i >= 0; --i) arg = v[i] == mx ? i : arg;
               list_offer(lk, li, nfill, thr, mx, col0 + arg);
             }
-          } else if (mx >= thr) {
-            // plain stores into this row's own list: no atomics, nothing to wait for
+          } else {
+            // one warp vote first: the common case (no row of the warp passes) skips the
+            // divergent region entirely
+            if (__any_sync(0xffffffffu, mx >= thr)) {
+              if (mx >= thr) {
+                // plain stores into this row's own list: no atomics, nothing to wait for
 #pragma unroll
-            for (int i = 0; i < 32; ++i)
-              if (v[i] >= thr) {
-                if (ncoll < a.list_len) {
-                  cid[ncoll] = col0 + i;
-                  ckey[ncoll] = v[i];
-                }
-                ++ncoll;
+                for (int i = 0; i < 32; ++i)
+                  if (v[i] >= thr) {
+                    if (ncoll < a.list_len) {
+                      cid[ncoll] = col0 + i;
+                      ckey[ncoll] = v[i];
+                    }
+                    ++ncoll;
+                  }
               }
+            }
           }
           __syncwarp();
           if (c + 1 < BN / HALVES / 32) tmem_ld_wait(ra);
         }
       }
       if (qvalid) {
-        if (a.mode == 0) {
+        if (MODE == 0) {
           for (int j = 0; j < nfill; ++j) {
             ckey[j] = lk[j];
             cid[j] = li[j];
@@ -993,7 +1004,6 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ga.n_chunks = s_chunks;
   ga.q_blocks = q_blocks;
   ga.stages = kb <= 2 ? 3 : 2;
-  ga.mode = 0;
   ga.per_column = s_tiles == n_tiles;
   ga.key_l2 = l2;
   ga.xnorm2 = s->xn.as<float>();
@@ -1005,8 +1015,9 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ga.q_active = s->qact.as<uint8_t>();
   ga.status = s->status.as<int32_t>();
   const int smem = SmemLayout(kb, ga.stages).total + 1024;
-  BF_CUDA(cudaFuncSetAttribute(bf16_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
-  bf16_scan_kernel<<<std::min(q_blocks * s_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, ga);
+  BF_CUDA(cudaFuncSetAttribute(bf16_scan_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
+  BF_CUDA(cudaFuncSetAttribute(bf16_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
+  bf16_scan_kernel<0><<<std::min(q_blocks * s_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, ga);
   BF_CUDA(cudaGetLastError(), "brute-force scan (sample)");
 
   RerankArgs ra;
@@ -1038,7 +1049,6 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   //    whose collection overflowed is scanned again with the raised tau of what it collected
   //    (up to three times: tau rises each time unless the collected keys are all tied).
   GemmArgs gb = ga;
-  gb.mode = 1;
   gb.per_column = 0;
   gb.n_tiles = n_tiles;
   gb.tile_step = 1;
@@ -1068,7 +1078,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   for (int attempt = 0; attempt < kScans; ++attempt) {
     BF_CUDA(cudaMemsetAsync(s->found.p, 0, nq * 4, st), "reset counts");
     BF_CUDA(cudaMemsetAsync(s->needs.p, 0, mpad, st), "reset flags");
-    bf16_scan_kernel<<<std::min(q_blocks * n_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, gb);
+    bf16_scan_kernel<1><<<std::min(q_blocks * n_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, gb);
     BF_CUDA(cudaGetLastError(), "brute-force scan");
     rb.only = attempt == 0 ? nullptr : s->qact.as<uint8_t>();  // the other queries keep their results
     rerank_kernel<<<rr_blocks, 256, 0, st>>>(rb);
