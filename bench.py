@@ -99,9 +99,13 @@ def index_path(m):
     return os.path.join(CACHE_DIR, f"{WORKLOAD}_M{m}_efc{EFC}_seed0.hnsw")
 
 
+HOST_BUILD_SECONDS = None
+
+
 def ensure_index(base, space, m, rank, world):
     """Rank 0 builds the index with the engine's host builder (all host cores) unless a copy is
     cached on this machine; the other ranks wait and load the same file."""
+    global HOST_BUILD_SECONDS
     from nmslib_b200 import SPACES, _capi
     path = index_path(m)
     if rank == 0 and not os.path.exists(path):
@@ -109,7 +113,8 @@ def ensure_index(base, space, m, rank, world):
         t0 = time.time()
         _capi.build_index(base, SPACES[space], m, EFC, nthreads=0, seed=0, out_path=path + ".tmp")
         os.replace(path + ".tmp", path)
-        log(f"[bench] built {path} in {time.time() - t0:.1f}s")
+        HOST_BUILD_SECONDS = time.time() - t0
+        log(f"[bench] built {path} in {HOST_BUILD_SECONDS:.1f}s")
     barrier(world)
     return path
 
@@ -291,6 +296,29 @@ def brute_force_measure(index, queries, k=10, reps=3):
            "qps": round(len(queries) / best), "tensor_tflops": round(flops / best / 1e12, 1),
            "sample_rows": int(st[0]), "max_rows_reranked": int(st[1]), "rescanned": int(st[2])}
     log(f"[bench] brute force: {res}")
+    return res
+
+
+def build_compare(base, space, m, queries, kth, host_recall, device):
+    """The same index built with the level-0 construction searches on the GPU: wall time and
+    recall@10 at the headline efSearch, beside the host build's."""
+    import nmslib_b200 as nmslib
+    from nmslib_b200 import SPACES, _capi
+    path = os.path.join(CACHE_DIR, f"{WORKLOAD}_M{m}_efc{EFC}_device_build.hnsw")
+    t0 = time.time()
+    _capi.build_index(base, SPACES[space], m, EFC, nthreads=0, seed=0, out_path=path, device=device)
+    dt = time.time() - t0
+    idx = nmslib.init(method="hnsw", space=space, device=device)
+    idx.loadIndex(path)
+    idx.setQueryTimeParams({"efSearch": HEADLINE_EF})
+    _, dd, cnt = idx.knnQueryBatchArrays(queries, K)
+    rec = recall_at_k(dd, cnt, kth, K)
+    del idx
+    os.remove(path)
+    res = {"host_build_s": None if HOST_BUILD_SECONDS is None else round(HOST_BUILD_SECONDS, 2),
+           "device_build_s": round(dt, 2), "host_threads": os.cpu_count(),
+           f"recall@10_ef{HEADLINE_EF}": {"host_build": round(host_recall, 4), "device_build": round(rec, 4)}}
+    log(f"[bench] index build: {res}")
     return res
 
 
@@ -575,6 +603,9 @@ def main():
     # ---- exact brute force on the tensor cores (same queries and vectors)
     brute = brute_force_measure(index, queries) if world == 1 else None
 
+    # ---- the index built again with the construction searches on the GPU
+    build_info = build_compare(base, space, m, queries, kth, head["recall@10"], local) if world == 1 else None
+
     peak, peak_kind = peaks()
     achieved = alg_bytes / (ms * 1e-3) / 1e9
     traffic = recorded_traffic()
@@ -607,7 +638,8 @@ def main():
                                                "visited_hash_log2": best_shape[2], "stage_rows": best_shape[3]},
                            "cuda_graph": True},
                 "serving": serving,
-                "bruteforce": brute}
+                "bruteforce": brute,
+                "index_build": build_info}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

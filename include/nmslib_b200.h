@@ -125,6 +125,19 @@ NMSG_API int nmsg_knn_batch(nmsg_index* index, const float* queries, int64_t nq,
 NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t dim, const int32_t* ids, int space, int M,
                               int ef_construction, int nthreads, uint64_t seed, const char* out_path);
 
+/* The same build with the efConstruction-wide level-0 searches on `device`: nodes with an upper
+ * level and the first 4096 nodes are inserted on the host as above; every other node (level 0
+ * only) joins in a batch whose searches run in the engine's search kernel (greedy descent, then
+ * the level-0 beam with ef = k = efConstruction) over the graph as it stands before the batch,
+ * after which the host selects its neighbours with heuristic 2 and adds the reverse links as
+ * Hnsw::add does (hnsw.cc:534-609). A batch is an eighth of the graph so far; its nodes do not see
+ * one another while searching. Same file format and parameters; the graph differs from a host
+ * build as two multi-threaded builds of the reference differ. No reference counterpart for the
+ * device part (the reference builds on the host only). */
+NMSG_API int nmsg_build_index_device(const float* data, int64_t n, int32_t dim, const int32_t* ids, int space, int M,
+                                     int ef_construction, int nthreads, uint64_t seed, int device,
+                                     const char* out_path);
+
 NMSG_API const char* nmsg_build_last_error(void);
 
 /* Launch shape of the search kernels; 0 in a field = chosen automatically. */

@@ -128,11 +128,12 @@ class FloatIndex:
 
     def createIndex(self, index_params=None, print_progress=False):
         """IndexWrapper::createIndex (nmslib.cc:89-96) -> Hnsw::CreateIndex (hnsw.cc:183-470),
-        built on the host by the engine's builder (M, efConstruction, indexThreadQty; maxM = M,
-        maxM0 = 2M, heuristic 2) and loaded onto the device."""
+        built by the engine's builder (M, efConstruction, indexThreadQty; maxM = M, maxM0 = 2M,
+        heuristic 2) and loaded onto the device. ``gpuBuild=1`` runs the level-0 construction
+        searches on this index's GPU (nmsg_build_index_device); the default builds on the host."""
         p = _load_params(index_params)
         known = {"M", "efConstruction", "indexThreadQty", "maxM", "maxM0", "delaunay_type", "post",
-                 "skip_optimized_index", "searchMethod", "seed"}
+                 "skip_optimized_index", "searchMethod", "seed", "gpuBuild"}
         if set(p) - known:
             raise RuntimeError("Unknown parameters found!")
         m = _as_int("M", p.get("M", "16"))
@@ -148,8 +149,10 @@ class FloatIndex:
         import tempfile
         with tempfile.TemporaryDirectory() as tmp:
             path = os.path.join(tmp, "index.hnsw")
+            gpu = _as_int("gpuBuild", p.get("gpuBuild", "0")) != 0
             _capi.build_index(data, SPACES[self.space], m, efc, ids=ids.astype(np.int32), nthreads=threads,
-                              seed=_as_int("seed", p.get("seed", "0")), out_path=path)
+                              seed=_as_int("seed", p.get("seed", "0")), out_path=path,
+                              device=self.device if gpu else None)
             self.loadIndex(path)
 
     def loadIndex(self, filename, load_data=False):

@@ -88,6 +88,9 @@ def load(path: str = LIB_PATH):
     lib.nmsg_build_index.argtypes = [P, I64, I32, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_uint64, ctypes.c_char_p]
     lib.nmsg_build_index.restype = ctypes.c_int
+    lib.nmsg_build_index_device.argtypes = [P, I64, I32, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_uint64, ctypes.c_int, ctypes.c_char_p]
+    lib.nmsg_build_index_device.restype = ctypes.c_int
     lib.nmsg_build_last_error.argtypes = []
     lib.nmsg_build_last_error.restype = ctypes.c_char_p
     lib.nmsg_last_error.argtypes = []
@@ -101,15 +104,19 @@ def last_error() -> str:
 
 
 def build_index(data, space: int, M: int = 16, ef_construction: int = 200, ids=None, nthreads: int = 0,
-                seed: int = 0, out_path: str = "index.hnsw"):
-    """Host HNSW build (nmsg_build_index) writing the reference's optimized file format."""
+                seed: int = 0, out_path: str = "index.hnsw", device=None):
+    """HNSW build writing the reference's optimized file format: on the host (nmsg_build_index),
+    or with the level-0 construction searches on GPU `device` (nmsg_build_index_device)."""
     import numpy as np
     lib = load()
     x = np.ascontiguousarray(data, dtype=np.float32)
     idv = None if ids is None else np.ascontiguousarray(ids, dtype=np.int32)
-    rc = lib.nmsg_build_index(x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1] if x.ndim == 2 else 0,
-                              None if idv is None else idv.ctypes.data_as(ctypes.c_void_p), space, M,
-                              ef_construction, nthreads, seed, os.fsencode(out_path))
+    args = (x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1] if x.ndim == 2 else 0,
+            None if idv is None else idv.ctypes.data_as(ctypes.c_void_p), space, M, ef_construction, nthreads, seed)
+    if device is None:
+        rc = lib.nmsg_build_index(*args, os.fsencode(out_path))
+    else:
+        rc = lib.nmsg_build_index_device(*args, int(device), os.fsencode(out_path))
     if rc != OK:
         msg = lib.nmsg_build_last_error().decode(errors="replace")
         raise (ValueError if rc == ERR_BAD_ARG else RuntimeError)(msg)

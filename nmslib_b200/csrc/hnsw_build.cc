@@ -23,7 +23,10 @@
 #include <thread>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "engine.h"
+#include "handle.h"
 #include "../../include/nmslib_b200.h"
 
 namespace nmsg {
@@ -89,7 +92,8 @@ struct Builder {
   double mult = 0;
   uint64_t seed = 0;
   std::vector<int32_t> level;
-  std::vector<int32_t> l0;                 // n x (maxM0 + 1): cnt, ids
+  int l0_stride = 40;                      // round_up(maxM0 + 1, 8): the device's level-0 pitch
+  std::vector<int32_t> l0;                 // n x l0_stride: cnt, ids
   std::vector<std::vector<int32_t>> up;    // per node: level x (maxM + 1)
   std::unique_ptr<SpinLock[]> locks;
   std::atomic<int32_t> enterpoint{0};
@@ -104,7 +108,7 @@ struct Builder {
     return space == NMSG_SPACE_COSINE ? 1.0f - d : -d;
   }
   int32_t* list(int64_t node, int lev) {
-    return lev == 0 ? l0.data() + node * (maxM0 + 1) : up[node].data() + (maxM + 1) * (lev - 1);
+    return lev == 0 ? l0.data() + node * l0_stride : up[node].data() + (maxM + 1) * (lev - 1);
   }
   int cap(int lev) const { return lev == 0 ? maxM0 : maxM; }
 
@@ -256,9 +260,11 @@ struct Builder {
 
 using namespace nmsg;
 
-extern "C" NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t dim, const int32_t* ids,
-                                         int space, int M, int ef_construction, int nthreads, uint64_t seed,
-                                         const char* out_path) {
+namespace nmsg {
+namespace {
+
+int check_build_args(const float* data, int64_t n, int32_t dim, int space, int M, int ef_construction,
+                     const char* out_path) {
   if (space == NMSG_SPACE_L1 || space == NMSG_SPACE_LINF) {
     g_build_err = "the host builder supports l2, cosinesimil and negdotprod; build l1 / linf indices with the reference";
     return NMSG_ERR_UNSUPPORTED;
@@ -267,25 +273,23 @@ extern "C" NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t d
     g_build_err = "invalid build arguments";
     return NMSG_ERR_BAD_ARG;
   }
-  HostIndex out;
-  std::string err;
-  if (n == 0) {
-    out.empty_regular = true;
-    int rc = write_index_file(out_path, out, err);
-    if (rc) g_build_err = err;
-    return rc;
-  }
   if (n > 0x7fffffffLL) {
     g_build_err = "too many elements for int32 ids";
     return NMSG_ERR_BAD_ARG;
   }
-  Builder b;
+  return NMSG_OK;
+}
+
+// Parameters, levels, empty lists and (cosine) the unit-vector copy, as CreateIndex sets them up.
+void setup_builder(Builder& b, const float* data, int64_t n, int32_t dim, int space, int M, int ef_construction,
+                   uint64_t seed) {
   b.n = n;
   b.dim = dim;
   b.space = space;
   b.M = M;
   b.maxM = M;
   b.maxM0 = 2 * M;
+  b.l0_stride = (b.maxM0 + 1 + 7) & ~7;
   b.efc = ef_construction;
   b.mult = 1.0 / std::log(1.0 * M);
   b.seed = seed;
@@ -313,26 +317,35 @@ extern "C" NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t d
     b.level[i] = b.random_level(i);
     if (b.level[i] > 0) b.up[i].assign((size_t)b.level[i] * (b.maxM + 1), 0);
   }
-  b.l0.assign((size_t)n * (b.maxM0 + 1), 0);
+  b.l0.assign((size_t)n * b.l0_stride, 0);
   b.locks.reset(new SpinLock[n]);
   b.enterpoint = 0;
   b.maxlevel = b.level[0];
-  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
-  std::atomic<int64_t> next(1);
+}
+
+// Inserts nodes[0..count) (all levels) with `nthreads` host threads, in list order.
+void insert_on_host(Builder& b, const int32_t* nodes, int64_t count, int nthreads) {
+  std::atomic<int64_t> next(0);
   auto worker = [&]() {
-    std::vector<uint32_t> vis(n, 0);
+    std::vector<uint32_t> vis(b.n, 0);
     uint32_t epoch = 0;
     for (;;) {
       const int64_t i = next.fetch_add(1);
-      if (i >= n) break;
-      b.add(i, vis, epoch);
+      if (i >= count) break;
+      b.add(nodes[i], vis, epoch);
     }
   };
   std::vector<std::thread> th;
   for (int t = 0; t < nthreads; ++t) th.emplace_back(worker);
   for (auto& t : th) t.join();
+}
 
-  // pack the optimized layout (hnsw.cc:353-465)
+// The optimized layout (hnsw.cc:353-465), written to out_path.
+int pack_and_write(const Builder& b, const int32_t* ids, const char* out_path) {
+  HostIndex out;
+  std::string err;
+  const int64_t n = b.n;
+  const int dim = b.dim, space = b.space;
   out.n = (uint32_t)n;
   out.dim = dim;
   out.maxM = (uint64_t)b.maxM;
@@ -358,7 +371,7 @@ extern "C" NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t d
     std::memcpy(row + 4, &label, 4);
     std::memcpy(row + 8, &dl, 8);
     std::memcpy(row + 16, b.data + i * dim, 4ull * dim);
-    const int32_t* lst = b.l0.data() + i * (b.maxM0 + 1);
+    const int32_t* lst = b.l0.data() + i * b.l0_stride;
     std::memcpy(row + out.off_level0, lst, 4ull * (1 + lst[0]));
     if (b.level[i] > 0) {
       out.up_off[i] = (int64_t)out.up_links.size();
@@ -369,6 +382,231 @@ extern "C" NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t d
   int rc = write_index_file(out_path, out, err);
   if (rc) g_build_err = err;
   return rc;
+}
+
+#define BUILD_CUDA(call, what)                                                                    \
+  do {                                                                                            \
+    const cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) {                                                                      \
+      g_build_err = std::string(what) + ": " + cudaGetErrorString(e_);                            \
+      return e_ == cudaErrorMemoryAllocation ? NMSG_ERR_OOM : NMSG_ERR_DEVICE;                    \
+    }                                                                                             \
+  } while (0)
+
+// Level-0 insertion of nodes[0..count) (level-0-only nodes) in batches. Each batch's
+// efConstruction-wide searches run on the device with the engine's search kernel (greedy descent
+// through the finished upper levels, then the level-0 beam with ef = efConstruction, k =
+// efConstruction) over the graph as it stands before the batch; the host then keeps each node's
+// neighbours with heuristic 2 and adds the reverse links exactly as `add` does (hnsw.cc:576-600,
+// hnsw.h:258-314), and the level-0 lists go back to the device. Nodes of one batch do not see one
+// another while they search (they are linked afterwards); a batch is an eighth of the graph so far.
+int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int device, int nthreads) {
+  if (count == 0) return NMSG_OK;
+  DeviceGuard guard(device);
+  int sms = 0;
+  BUILD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device query");
+  const int64_t n = b.n;
+  const int dim = b.dim;
+  DevIndex d;
+  d.n = n;
+  d.dim = dim;
+  d.pitch = (dim + 31) & ~31;
+  d.n16 = dim & ~15;
+  d.n4 = dim & ~3;
+  d.maxM = b.maxM;
+  d.maxM0 = b.maxM0;
+  d.l0_pitch = b.l0_stride;
+  d.maxlevel = b.maxlevel.load();
+  d.enterpoint = b.enterpoint.load();
+  d.dist_type = b.space == NMSG_SPACE_L2 ? (dim % 16 == 0 ? kL2Sqr16Ext : kL2SqrExt)
+                                         : (b.space == NMSG_SPACE_COSINE ? kNormCosine : kNegDot);
+  // vectors in the search kernels' permuted layout, upper levels as CSR, identity ids (the kernel
+  // then reports internal node numbers)
+  std::vector<float> vec((size_t)n * d.pitch, 0.0f);
+  std::vector<int64_t> up_off(n, -1);
+  std::vector<int32_t> up_links;
+  std::vector<int32_t> ident(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const float* src = b.data + i * dim;
+    float* dst = vec.data() + i * d.pitch;
+    for (int e = 0; e < dim; ++e) dst[permuted_pos(e, dim)] = src[e];
+    if (b.level[i] > 0) {
+      up_off[i] = (int64_t)up_links.size();
+      up_links.insert(up_links.end(), b.up[i].begin(), b.up[i].end());
+    }
+    ident[i] = (int32_t)i;
+  }
+  if (up_links.empty()) up_links.push_back(0);
+  DevBuf g_vec, g_l0, g_off, g_links, g_ext, g_q, g_ids, g_d, g_cnt, g_vis, g_ep, g_counter, g_status;
+  struct Release {
+    std::vector<DevBuf*> bufs;
+    ~Release() {
+      for (DevBuf* p : bufs) p->release();
+    }
+  } release{{&g_vec, &g_l0, &g_off, &g_links, &g_ext, &g_q, &g_ids, &g_d, &g_cnt, &g_vis, &g_ep, &g_counter, &g_status}};
+  BUILD_CUDA(g_vec.ensure(vec.size() * 4, false), "cudaMalloc(vectors)");
+  BUILD_CUDA(g_l0.ensure(b.l0.size() * 4, false), "cudaMalloc(level-0 lists)");
+  BUILD_CUDA(g_off.ensure(n * 8, false), "cudaMalloc(upper offsets)");
+  BUILD_CUDA(g_links.ensure(up_links.size() * 4, false), "cudaMalloc(upper lists)");
+  BUILD_CUDA(g_ext.ensure(n * 4, false), "cudaMalloc(ids)");
+  BUILD_CUDA(cudaMemcpy(g_vec.p, vec.data(), vec.size() * 4, cudaMemcpyHostToDevice), "upload vectors");
+  BUILD_CUDA(cudaMemcpy(g_off.p, up_off.data(), n * 8, cudaMemcpyHostToDevice), "upload offsets");
+  BUILD_CUDA(cudaMemcpy(g_links.p, up_links.data(), up_links.size() * 4, cudaMemcpyHostToDevice), "upload links");
+  BUILD_CUDA(cudaMemcpy(g_ext.p, ident.data(), n * 4, cudaMemcpyHostToDevice), "upload ids");
+  vec.clear();
+  vec.shrink_to_fit();
+  d.vecs = g_vec.as<float>();
+  d.l0 = g_l0.as<int32_t>();
+  d.up_off = g_off.as<int64_t>();
+  d.up_links = g_links.as<int32_t>();
+  d.ext_id = g_ext.as<int32_t>();
+
+  const int efc = b.efc;
+  LaunchPlan plan;
+  std::string perr;
+  const nmsg_launch_config cfg{0, 0, 0, 0};
+  int rc = plan_launch(d, cfg, efc, false, false, &plan, &perr);
+  if (rc != NMSG_OK) {
+    g_build_err = "device build: " + perr;
+    return rc;
+  }
+  const int blocks = plan.blocks_per_sm * sms;
+  const int slots = blocks * plan.wpb;
+  const int64_t vpitch = ((n + 15) / 16) * 16;
+  const int64_t max_batch = 65536;
+  BUILD_CUDA(g_vis.ensure((size_t)slots * vpitch, true), "cudaMalloc(visited sets)");
+  BUILD_CUDA(g_ep.ensure(slots, true), "cudaMalloc(epochs)");
+  BUILD_CUDA(g_counter.ensure(4, true), "cudaMalloc(counter)");
+  BUILD_CUDA(g_status.ensure(4, true), "cudaMalloc(status)");
+  BUILD_CUDA(g_q.ensure((size_t)max_batch * dim * 4, false), "cudaMalloc(queries)");
+  BUILD_CUDA(g_ids.ensure((size_t)max_batch * efc * 4, false), "cudaMalloc(results)");
+  BUILD_CUDA(g_d.ensure((size_t)max_batch * efc * 4, false), "cudaMalloc(results)");
+  BUILD_CUDA(g_cnt.ensure((size_t)max_batch * 4, false), "cudaMalloc(results)");
+
+  SearchArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.ix = d;
+  a.k_default = efc;
+  a.ef_default = efc;
+  a.algo = NMSG_ALGO_V1MERGE;
+  a.kmax = efc;
+  a.queries = g_q.as<float>();
+  a.ids = g_ids.as<int32_t>();
+  a.dists = g_d.as<float>();
+  a.counts = g_cnt.as<int32_t>();
+  a.visited = g_vis.as<uint8_t>();
+  a.visited_pitch = vpitch;
+  a.epochs = g_ep.as<uint8_t>();
+  a.num_slots = slots;
+  a.work_counter = g_counter.as<int32_t>();
+  a.status = g_status.as<int32_t>();
+  a.region_items = plan.region;
+  a.nbpad = plan.nbpad;
+  a.hash_log2 = plan.hash_log2;
+  a.stage_rows = plan.stage_rows;
+  a.warp_smem = plan.warp_smem;
+
+  std::vector<float> hq((size_t)max_batch * dim);
+  std::vector<int32_t> hids((size_t)max_batch * efc), hcnt(max_batch);
+  std::vector<float> hd((size_t)max_batch * efc);
+  int64_t inserted = n - count, done = 0;
+  while (done < count) {
+    const int64_t bsz = std::min<int64_t>({count - done, max_batch, std::max<int64_t>(1024, inserted / 8)});
+    const int32_t* batch = nodes + done;
+    for (int64_t j = 0; j < bsz; ++j) std::memcpy(hq.data() + j * dim, b.data + (int64_t)batch[j] * dim, 4ull * dim);
+    BUILD_CUDA(cudaMemcpy(g_l0.p, b.l0.data(), b.l0.size() * 4, cudaMemcpyHostToDevice), "upload lists");
+    BUILD_CUDA(cudaMemcpy(g_q.p, hq.data(), (size_t)bsz * dim * 4, cudaMemcpyHostToDevice), "upload queries");
+    a.nq = bsz;
+    BUILD_CUDA(cudaMemset(g_counter.p, 0, 4), "reset counter");
+    BUILD_CUDA(cudaMemset(g_status.p, 0, 4), "reset status");
+    const int lrc = launch_search(a, false, plan.gather, false, blocks, plan.wpb, nullptr);
+    if (lrc != 0) {
+      g_build_err = std::string("device build search launch: ") + cudaGetErrorString((cudaError_t)lrc);
+      return NMSG_ERR_DEVICE;
+    }
+    BUILD_CUDA(cudaMemcpy(hids.data(), g_ids.p, (size_t)bsz * efc * 4, cudaMemcpyDeviceToHost), "copy results");
+    BUILD_CUDA(cudaMemcpy(hd.data(), g_d.p, (size_t)bsz * efc * 4, cudaMemcpyDeviceToHost), "copy results");
+    BUILD_CUDA(cudaMemcpy(hcnt.data(), g_cnt.p, (size_t)bsz * 4, cudaMemcpyDeviceToHost), "copy results");
+    int32_t status = 0;
+    BUILD_CUDA(cudaMemcpy(&status, g_status.p, 4, cudaMemcpyDeviceToHost), "copy status");
+    if (status != 0) {
+      g_build_err = "device build: the search kernel reported status " + std::to_string(status);
+      return status;
+    }
+    // neighbour selection and links, as in `add` at level 0
+    std::atomic<int64_t> next(0);
+    auto worker = [&]() {
+      std::vector<std::pair<float, int32_t>> res;
+      for (;;) {
+        const int64_t j = next.fetch_add(1);
+        if (j >= bsz) break;
+        const int32_t node = batch[j];
+        res.clear();
+        for (int t = 0; t < hcnt[j]; ++t) res.push_back({hd[j * efc + t], hids[j * efc + t]});
+        b.heuristic(res, b.M);
+        std::sort(res.begin(), res.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        for (const auto& r : res) {
+          b.add_friend(r.second, 0, node);
+          b.add_friend(node, 0, r.second);
+        }
+      }
+    };
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; ++t) th.emplace_back(worker);
+    for (auto& t : th) t.join();
+    done += bsz;
+    inserted += bsz;
+  }
+  return NMSG_OK;
+}
+
+int write_empty(const char* out_path) {
+  HostIndex out;
+  std::string err;
+  out.empty_regular = true;
+  int rc = write_index_file(out_path, out, err);
+  if (rc) g_build_err = err;
+  return rc;
+}
+
+}  // namespace
+}  // namespace nmsg
+
+using namespace nmsg;
+
+extern "C" NMSG_API int nmsg_build_index(const float* data, int64_t n, int32_t dim, const int32_t* ids,
+                                         int space, int M, int ef_construction, int nthreads, uint64_t seed,
+                                         const char* out_path) {
+  int rc = check_build_args(data, n, dim, space, M, ef_construction, out_path);
+  if (rc != NMSG_OK) return rc;
+  if (n == 0) return write_empty(out_path);
+  Builder b;
+  setup_builder(b, data, n, dim, space, M, ef_construction, seed);
+  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  std::vector<int32_t> order(n - 1);
+  for (int64_t i = 1; i < n; ++i) order[i - 1] = (int32_t)i;  // node 0 is the initial entry point
+  insert_on_host(b, order.data(), n - 1, nthreads);
+  return pack_and_write(b, ids, out_path);
+}
+
+extern "C" NMSG_API int nmsg_build_index_device(const float* data, int64_t n, int32_t dim, const int32_t* ids,
+                                                int space, int M, int ef_construction, int nthreads, uint64_t seed,
+                                                int device, const char* out_path) {
+  int rc = check_build_args(data, n, dim, space, M, ef_construction, out_path);
+  if (rc != NMSG_OK) return rc;
+  if (n == 0) return write_empty(out_path);
+  Builder b;
+  setup_builder(b, data, n, dim, space, M, ef_construction, seed);
+  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  // on the host: every node with an upper level and the first nodes, in node order; the rest
+  // (level 0 only) in device-searched batches
+  const int64_t head = std::min<int64_t>(n, 4096);
+  std::vector<int32_t> host_nodes, dev_nodes;
+  for (int64_t i = 1; i < n; ++i) (i < head || b.level[i] > 0 ? host_nodes : dev_nodes).push_back((int32_t)i);
+  insert_on_host(b, host_nodes.data(), (int64_t)host_nodes.size(), nthreads);
+  rc = insert_level0_on_device(b, dev_nodes.data(), (int64_t)dev_nodes.size(), device, nthreads);
+  if (rc != NMSG_OK) return rc;
+  return pack_and_write(b, ids, out_path);
 }
 
 extern "C" NMSG_API const char* nmsg_build_last_error(void) { return g_build_err.c_str(); }
