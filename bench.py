@@ -278,8 +278,9 @@ def serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6), seconds=1.0, seed
 
 
 def brute_force_measure(index, queries, k=10, reps=3):
-    """Exact k-NN of the whole batch over every stored vector (tcgen05 BF16 GEMM + exact rerank):
-    time and tensor throughput (2 * nq * n * padded dim FLOP per batch)."""
+    """Exact k-NN of the whole batch over every stored vector: time and throughput. The tensor-core
+    path (l2 / cosine / negdot, dim <= 256) reports 2 * nq * n * padded dim BF16 FLOP per batch; the
+    exact CUDA-core scan (L1, LInf, wider rows) 2 * nq * n * dim FP32 FLOP."""
     import torch
     ids, d, c, st = index.bruteForceBatchArrays(queries, k, stats=True)  # builds the BF16 copy
     t = []
@@ -290,11 +291,17 @@ def brute_force_measure(index, queries, k=10, reps=3):
         t.append(time.perf_counter() - t0)
     best = min(t)
     n, dim = index.info["n"], index.info["dim"]
-    kp = (dim + 63) // 64 * 64
-    flops = 2.0 * len(queries) * n * kp
-    res = {"queries": len(queries), "k": k, "ms_end_to_end": round(best * 1e3, 3),
-           "qps": round(len(queries) / best), "tensor_tflops": round(flops / best / 1e12, 1),
-           "sample_rows": int(st[0]), "max_rows_reranked": int(st[1]), "rescanned": int(st[2])}
+    if st[0] == 0:  # the exact CUDA-core scan
+        flops = 2.0 * len(queries) * n * dim
+        res = {"path": "exact CUDA-core scan", "queries": len(queries), "k": k, "ms_end_to_end": round(best * 1e3, 3),
+               "qps": round(len(queries) / best), "fp32_tflops": round(flops / best / 1e12, 1)}
+    else:
+        kp = (dim + 63) // 64 * 64
+        flops = 2.0 * len(queries) * n * kp
+        res = {"path": "tensor-core BF16 + exact rerank", "queries": len(queries), "k": k,
+               "ms_end_to_end": round(best * 1e3, 3), "qps": round(len(queries) / best),
+               "tensor_tflops": round(flops / best / 1e12, 1), "sample_rows": int(st[0]),
+               "max_rows_reranked": int(st[1]), "rescanned": int(st[2])}
     log(f"[bench] brute force: {res}")
     return res
 
@@ -410,6 +417,7 @@ def run_aux(args):
         dt, (ids, d, cnt) = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
         # recall@k per query against the float64 k-th distance of that query's own k
         kth_k = np.array([fp for fp in kth])  # k = 100 column; per-k recall below uses the row's own k
+        out["bruteforce"] = brute_force_measure(index, queries[:1000])
         out["mixed_batch"] = {"queries": nq, "qps_e2e": round(nq / dt), "ms": round(dt * 1e3, 2),
                               "searchold_queries": int((ef >= 1000).sum())}
         truth10 = fp64_truth(base, queries, 10, space)

@@ -177,7 +177,10 @@ NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* index, const float* queries, int
  * reaches; a second BF16 GEMM over the whole base collects the vectors at or above it and the
  * exact rerank orders them. The ids are the exact top-k (ties by id); distances follow the
  * index's space as the HNSW path reports them (squared L2, 1 - cos on normalised vectors, -dot).
- * dim <= 256, k <= 32. The full scan keeps up to 64 vectors per query and per half of a base
+ * k <= 32. That is the path for l2 / cosinesimil / negdotprod with dim <= 256; L1, LInf and wider
+ * rows are scanned exactly on CUDA cores with the query path's own distance arithmetic (every
+ * distance bit-identical to the HNSW search's; stats then {0, n, 0, chunks}). The full scan keeps
+ * up to 64 vectors per query and per half of a base
  * chunk; a query that finds more in some chunk is scanned again with a raised threshold (up to
  * three times), and if it still overflows the call returns NMSG_ERR_CAPACITY (many vectors tied
  * with the k-th neighbour within the BF16 error bound). stats (optional, 4 values): sample rows

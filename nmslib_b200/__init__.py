@@ -261,7 +261,9 @@ class FloatIndex:
 
     def bruteForceBatchArrays(self, queries, k=10, stats=False):
         """Exact k-NN over every stored vector (seq_search semantics) on the tensor cores:
-        (ids [nq, k] external, dists [nq, k], counts [nq][, stats [4]]). k <= 32, dim <= 256."""
+        (ids [nq, k] external, dists [nq, k], counts [nq][, stats [4]]). k <= 32. l2 / cosinesimil /
+        negdotprod rows of up to 256 floats use BF16 tensor cores with an exact rerank; L1, LInf
+        and wider rows an exact CUDA-core scan."""
         h = self._require()
         q = self._queries(queries)
         nq = q.shape[0]

@@ -878,6 +878,54 @@ int prepare_base(nmsg_index* h, BruteForceState* s) {
   return NMSG_OK;
 }
 
+// L1 / LInf and rows wider than 256: every distance exactly as the search computes it, on CUDA
+// cores (exact_scan_knn); stats = {0, rows scanned per query, 0, base chunks per query block}.
+int scan_fallback(nmsg_index* h, const float* queries, int64_t nq, int dim, int k, int kmax, int32_t* ids, float* dists,
+                  int32_t* counts, int64_t* stats, bool dev_ptrs, cudaStream_t st) {
+  BruteForceState* s = h->bf ? h->bf : (h->bf = new BruteForceState());
+  const DevIndex& d = h->dev;
+  const int64_t q_blocks = (nq + 7) / 8;
+  const int n_chunks = (int)std::max<int64_t>(
+      1, std::min<int64_t>((4 * h->num_sms + q_blocks - 1) / q_blocks, std::max<int64_t>(1, d.n / 2048)));
+  const float* qin = queries;
+  if (!dev_ptrs) {
+    BF_CUDA(s->h_q.ensure((size_t)nq * dim * 4, false), "cudaMalloc(query staging)");
+    BF_CUDA(cudaMemcpyAsync(s->h_q.p, queries, (size_t)nq * dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
+    qin = s->h_q.as<float>();
+  }
+  BF_CUDA(s->scr_key.ensure((size_t)nq * n_chunks * k * 4, false), "cudaMalloc(scan lists)");
+  BF_CUDA(s->scr_id.ensure((size_t)nq * n_chunks * k * 4, false), "cudaMalloc(scan lists)");
+  int32_t* o_ids = ids;
+  float* o_d = dists;
+  int32_t* o_c = counts;
+  if (!dev_ptrs) {
+    BF_CUDA(s->h_ids.ensure((size_t)nq * kmax * 4, false), "cudaMalloc(staging)");
+    BF_CUDA(s->h_dists.ensure((size_t)nq * kmax * 4, false), "cudaMalloc(staging)");
+    BF_CUDA(s->h_counts.ensure(nq * 4, false), "cudaMalloc(staging)");
+    o_ids = s->h_ids.as<int32_t>();
+    o_d = s->h_dists.as<float>();
+    o_c = s->h_counts.as<int32_t>();
+  }
+  const int rc = exact_scan_knn(d, qin, nq, k, kmax, s->scr_key.as<float>(), s->scr_id.as<int32_t>(), n_chunks, o_ids,
+                                o_d, o_c, st);
+  if (rc != 0)
+    return bf_fail(NMSG_ERR_DEVICE, std::string("exact scan: ") + cudaGetErrorString((cudaError_t)rc) +
+                                        (rc == (int)cudaErrorInvalidValue ? " (rows too wide for the scan)" : ""));
+  if (!dev_ptrs) {
+    BF_CUDA(cudaMemcpyAsync(ids, o_ids, (size_t)nq * kmax * 4, cudaMemcpyDeviceToHost, st), "copy ids");
+    BF_CUDA(cudaMemcpyAsync(dists, o_d, (size_t)nq * kmax * 4, cudaMemcpyDeviceToHost, st), "copy distances");
+    BF_CUDA(cudaMemcpyAsync(counts, o_c, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
+  }
+  BF_CUDA(cudaStreamSynchronize(st), "exact scan");
+  if (stats) {
+    stats[0] = 0;
+    stats[1] = d.n;
+    stats[2] = 0;
+    stats[3] = n_chunks;
+  }
+  return NMSG_OK;
+}
+
 }  // namespace
 }  // namespace nmsg
 
@@ -889,8 +937,6 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   if (!h) return bf_fail(NMSG_ERR_BAD_ARG, "Must call createIndex or loadIndex before this method");
   if (nq < 0 || k < 1 || kmax < k) return bf_fail(NMSG_ERR_BAD_ARG, "nq must be >= 0, k >= 1 and kmax >= k");
   if (k > CAND) return bf_fail(NMSG_ERR_UNSUPPORTED, "brute force supports k <= 32");
-  if (h->space != NMSG_SPACE_L2 && h->space != NMSG_SPACE_COSINE && h->space != NMSG_SPACE_NEGDOT)
-    return bf_fail(NMSG_ERR_UNSUPPORTED, "brute force on the tensor cores supports l2, cosinesimil and negdotprod");
   if (nq > 0 && (!queries || !ids || !dists || !counts)) return bf_fail(NMSG_ERR_BAD_ARG, "null buffer");
   std::lock_guard<std::mutex> lk(h->mu);
   const bool dev_ptrs = flags & NMSG_DEVICE_PTRS;
@@ -905,9 +951,11 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
     return NMSG_OK;
   }
   if (dim != hi.dim) return bf_fail(NMSG_ERR_BAD_ARG, "query dimension does not match the index dimension");
-  if (((dim + BK - 1) / BK) > KB_MAX) return bf_fail(NMSG_ERR_UNSUPPORTED, "brute force supports dim <= 256");
   DeviceGuard g(h->device);
   cudaStream_t st = (cudaStream_t)stream;
+  const bool dot_space = h->space == NMSG_SPACE_L2 || h->space == NMSG_SPACE_COSINE || h->space == NMSG_SPACE_NEGDOT;
+  if (!dot_space || ((dim + BK - 1) / BK) > KB_MAX)
+    return scan_fallback(h, queries, nq, dim, k, kmax, ids, dists, counts, stats, dev_ptrs, st);
   if (!h->bf) {
     h->bf = new BruteForceState();
     const int rc = prepare_base(h, h->bf);
@@ -1015,8 +1063,8 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ga.q_active = s->qact.as<uint8_t>();
   ga.status = s->status.as<int32_t>();
   const int smem = SmemLayout(kb, ga.stages).total + 1024;
-  BF_CUDA(cudaFuncSetAttribute(bf16_scan_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
-  BF_CUDA(cudaFuncSetAttribute(bf16_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
+  BF_CUDA((cudaError_t)allow_max_smem((const void*)bf16_scan_kernel<0>), "smem attribute");
+  BF_CUDA((cudaError_t)allow_max_smem((const void*)bf16_scan_kernel<1>), "smem attribute");
   bf16_scan_kernel<0><<<std::min(q_blocks * s_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, ga);
   BF_CUDA(cudaGetLastError(), "brute-force scan (sample)");
 

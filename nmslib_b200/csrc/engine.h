@@ -123,6 +123,30 @@ int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int hash_lo
 // Return a cudaError_t value.
 int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, int blocks, int warps_per_block,
                   void* stream);
+
+// Opt-in dynamic shared memory of the current device (227 KB on B200).
+constexpr int kMaxDynamicSmem = 227 * 1024;
+
+// Lets `kern` launch with up to kMaxDynamicSmem of dynamic shared memory, once per device and
+// kernel. The limit is a process-wide property of the function, so it is raised once and never
+// set per launch: a per-launch value would race with launches of the same kernel from other
+// threads (serving lanes, concurrent callers) that need more. Returns a cudaError_t value.
+int allow_max_smem(const void* kern);
+// Exact k-NN (k <= 32) by scanning every row with the query path's distance arithmetic, on CUDA
+// cores (hnsw_search.cu): rows split into n_chunks per query block; part_d / part_id are
+// [nq][n_chunks][k] scratch. Outputs as the search writes them (external ids, -1 / +inf padding).
+// Returns a cudaError_t value.
+int exact_scan_knn(const DevIndex& ix, const float* queries, int64_t nq, int k, int kmax, float* part_d,
+                   int32_t* part_id, int n_chunks, int32_t* ids, float* dists, int32_t* counts, void* stream);
+
+// Device-assisted build (build_gpu.cu): heuristic-2 selection for a searched batch of new nodes,
+// their lists, and the reverse links merged into their neighbours' lists (maxM0 <= 64). pend /
+// pend_cnt ([n][32] / [n], zero at the first call) and touched ([nb * M]) are scratch. Returns a
+// cudaError_t value.
+int level0_select_and_link(const DevIndex& ix, int space, int M, int efc, int64_t nb, const int32_t* nodes,
+                           const int32_t* cand_ids, const float* cand_d, const int32_t* cand_cnt, int32_t* l0,
+                           int32_t* pend, int32_t* pend_cnt, int32_t* touched, int32_t* n_touched, void* stream);
+
 int search_occupancy(bool plain, int gather, bool with_old, int warps_per_block, int smem_per_block,
                      int* blocks_per_sm);
 

@@ -396,9 +396,11 @@ int pack_and_write(const Builder& b, const int32_t* ids, const char* out_path) {
 // Level-0 insertion of nodes[0..count) (level-0-only nodes) in batches. Each batch's
 // efConstruction-wide searches run on the device with the engine's search kernel (greedy descent
 // through the finished upper levels, then the level-0 beam with ef = efConstruction, k =
-// efConstruction) over the graph as it stands before the batch; the host then keeps each node's
-// neighbours with heuristic 2 and adds the reverse links exactly as `add` does (hnsw.cc:576-600,
-// hnsw.h:258-314), and the level-0 lists go back to the device. Nodes of one batch do not see one
+// efConstruction) over the graph as it stands before the batch; then each node's neighbours are
+// kept with heuristic 2 and the reverse links added as `add` does (hnsw.cc:576-600,
+// hnsw.h:258-314) — on the device (build_gpu.cu, the level-0 graph stays there for the whole
+// phase) for l2 and cosine with maxM0 <= 64, else on the host with the lists uploaded again per
+// batch. Nodes of one batch do not see one
 // another while they search (they are linked afterwards); a batch is an eighth of the graph so far.
 int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int device, int nthreads) {
   if (count == 0) return NMSG_OK;
@@ -437,13 +439,20 @@ int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int
     ident[i] = (int32_t)i;
   }
   if (up_links.empty()) up_links.push_back(0);
-  DevBuf g_vec, g_l0, g_off, g_links, g_ext, g_q, g_ids, g_d, g_cnt, g_vis, g_ep, g_counter, g_status;
+  DevBuf g_vec, g_l0, g_off, g_links, g_ext, g_q, g_ids, g_d, g_cnt, g_vis, g_ep, g_counter, g_status, g_nodes, g_pend,
+      g_pend_cnt, g_touched, g_ntouched;
   struct Release {
     std::vector<DevBuf*> bufs;
     ~Release() {
       for (DevBuf* p : bufs) p->release();
     }
-  } release{{&g_vec, &g_l0, &g_off, &g_links, &g_ext, &g_q, &g_ids, &g_d, &g_cnt, &g_vis, &g_ep, &g_counter, &g_status}};
+  } release{{&g_vec, &g_l0, &g_off, &g_links, &g_ext, &g_q, &g_ids, &g_d, &g_cnt, &g_vis, &g_ep, &g_counter, &g_status,
+             &g_nodes, &g_pend, &g_pend_cnt, &g_touched, &g_ntouched}};
+  // neighbour selection and links run on the device too when the lists fit its kernels, except
+  // for negative dot product: there a few high-norm nodes are the nearest neighbours of nearly
+  // every node and receive thousands of links per batch, more than the device's per-neighbour
+  // queue keeps (the host path weighs each of them; measured recall@10 0.908 instead of 0.941)
+  const bool link_on_device = b.maxM0 <= 64 && b.space != NMSG_SPACE_NEGDOT;
   BUILD_CUDA(g_vec.ensure(vec.size() * 4, false), "cudaMalloc(vectors)");
   BUILD_CUDA(g_l0.ensure(b.l0.size() * 4, false), "cudaMalloc(level-0 lists)");
   BUILD_CUDA(g_off.ensure(n * 8, false), "cudaMalloc(upper offsets)");
@@ -482,6 +491,14 @@ int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int
   BUILD_CUDA(g_ids.ensure((size_t)max_batch * efc * 4, false), "cudaMalloc(results)");
   BUILD_CUDA(g_d.ensure((size_t)max_batch * efc * 4, false), "cudaMalloc(results)");
   BUILD_CUDA(g_cnt.ensure((size_t)max_batch * 4, false), "cudaMalloc(results)");
+  if (link_on_device) {
+    BUILD_CUDA(g_nodes.ensure((size_t)max_batch * 4, false), "cudaMalloc(batch)");
+    BUILD_CUDA(g_pend.ensure((size_t)n * 32 * 4, false), "cudaMalloc(queued links)");
+    BUILD_CUDA(g_pend_cnt.ensure((size_t)n * 4, true), "cudaMalloc(queued links)");
+    BUILD_CUDA(g_touched.ensure((size_t)max_batch * b.M * 4, false), "cudaMalloc(queued links)");
+    BUILD_CUDA(g_ntouched.ensure(4, true), "cudaMalloc(queued links)");
+    BUILD_CUDA(cudaMemcpy(g_l0.p, b.l0.data(), b.l0.size() * 4, cudaMemcpyHostToDevice), "upload lists");
+  }
 
   SearchArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -514,7 +531,8 @@ int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int
     const int64_t bsz = std::min<int64_t>({count - done, max_batch, std::max<int64_t>(1024, inserted / 8)});
     const int32_t* batch = nodes + done;
     for (int64_t j = 0; j < bsz; ++j) std::memcpy(hq.data() + j * dim, b.data + (int64_t)batch[j] * dim, 4ull * dim);
-    BUILD_CUDA(cudaMemcpy(g_l0.p, b.l0.data(), b.l0.size() * 4, cudaMemcpyHostToDevice), "upload lists");
+    if (!link_on_device)
+      BUILD_CUDA(cudaMemcpy(g_l0.p, b.l0.data(), b.l0.size() * 4, cudaMemcpyHostToDevice), "upload lists");
     BUILD_CUDA(cudaMemcpy(g_q.p, hq.data(), (size_t)bsz * dim * 4, cudaMemcpyHostToDevice), "upload queries");
     a.nq = bsz;
     BUILD_CUDA(cudaMemset(g_counter.p, 0, 4), "reset counter");
@@ -523,6 +541,26 @@ int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int
     if (lrc != 0) {
       g_build_err = std::string("device build search launch: ") + cudaGetErrorString((cudaError_t)lrc);
       return NMSG_ERR_DEVICE;
+    }
+    if (link_on_device) {
+      BUILD_CUDA(cudaMemcpy(g_nodes.p, batch, (size_t)bsz * 4, cudaMemcpyHostToDevice), "upload batch");
+      const int lrc2 = level0_select_and_link(d, b.space, b.M, efc, bsz, g_nodes.as<int32_t>(), g_ids.as<int32_t>(),
+                                              g_d.as<float>(), g_cnt.as<int32_t>(), g_l0.as<int32_t>(),
+                                              g_pend.as<int32_t>(), g_pend_cnt.as<int32_t>(),
+                                              g_touched.as<int32_t>(), g_ntouched.as<int32_t>(), nullptr);
+      if (lrc2 != 0) {
+        g_build_err = std::string("device build linking: ") + cudaGetErrorString((cudaError_t)lrc2);
+        return NMSG_ERR_DEVICE;
+      }
+      int32_t status = 0;
+      BUILD_CUDA(cudaMemcpy(&status, g_status.p, 4, cudaMemcpyDeviceToHost), "copy status");
+      if (status != 0) {
+        g_build_err = "device build: the search kernel reported status " + std::to_string(status);
+        return status;
+      }
+      done += bsz;
+      inserted += bsz;
+      continue;
     }
     BUILD_CUDA(cudaMemcpy(hids.data(), g_ids.p, (size_t)bsz * efc * 4, cudaMemcpyDeviceToHost), "copy results");
     BUILD_CUDA(cudaMemcpy(hd.data(), g_d.p, (size_t)bsz * efc * 4, cudaMemcpyDeviceToHost), "copy results");
@@ -557,6 +595,8 @@ int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int
     done += bsz;
     inserted += bsz;
   }
+  if (link_on_device)
+    BUILD_CUDA(cudaMemcpy(b.l0.data(), g_l0.p, b.l0.size() * 4, cudaMemcpyDeviceToHost), "download lists");
   return NMSG_OK;
 }
 

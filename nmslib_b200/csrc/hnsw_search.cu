@@ -21,6 +21,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "engine.h"
 #include "../../include/nmslib_b200.h"
 
@@ -1206,7 +1211,200 @@ __global__ void __launch_bounds__(32, 32) search_plain_kernel(SearchArgs a) {
   if (lane == 0) atomicExch(a.slot_locks + slot, 0);
 }
 
+// ------------------------------------------------------------------ exact scan on CUDA cores
+// Exact k-NN (SeqSearch semantics, similarity_search/src/method/seqsearch.cc:143-177) for what the
+// tensor-core brute force does not take: L1 / LInf and rows wider than 256. A block of kScanWarps
+// warps owns kScanWarps queries and one chunk of base rows; the rows are staged into shared memory
+// a round at a time and every warp computes its query's distances with the query path's own
+// arithmetic (so each distance is the value the HNSW search reports), keeping its best k by
+// (distance, row) in a lane-distributed sorted list. scan_merge_kernel merges the chunks.
+constexpr int kScanWarps = 8;
+
+__device__ __forceinline__ bool scan_better(float da, int ia, float db, int ib) {
+  return da < db || (da == db && ia < ib);
+}
+
+// Offers (d, row) to the warp's sorted list (lane i < k holds the i-th best); warp-uniform inputs.
+__device__ __forceinline__ void scan_offer(float& bd, int& bi, int k, float d, int row) {
+  const int lane = lane_id();
+  const float kd = __shfl_sync(kFull, bd, k - 1);
+  const int ki = __shfl_sync(kFull, bi, k - 1);
+  if (!scan_better(d, row, kd, ki)) return;
+  const int pos = __popc(__ballot_sync(kFull, lane < k && scan_better(bd, bi, d, row)));
+  const float ud = __shfl_up_sync(kFull, bd, 1);
+  const int ui = __shfl_up_sync(kFull, bi, 1);
+  if (lane > pos && lane < k) {
+    bd = ud;
+    bi = ui;
+  } else if (lane == pos) {
+    bd = d;
+    bi = row;
+  }
+}
+
+struct ScanArgs {
+  DevIndex ix;
+  const float* queries;  // [nq][dim]
+  int64_t nq;
+  int k;                 // <= 32
+  int64_t chunk_rows;
+  int n_chunks;
+  int stage_rows;        // rows per staged round (multiple of 4)
+  float* part_d;         // [nq][n_chunks][k]
+  int32_t* part_id;
+};
+
+__global__ void __launch_bounds__(32 * kScanWarps) exact_scan_kernel(ScanArgs a) {
+  extern __shared__ __align__(16) float scan_smem[];
+  const DevIndex& ix = a.ix;
+  const int warp = threadIdx.x >> 5, lane = lane_id(), g = lane >> 3, j = lane & 7;
+  float* rows = scan_smem;  // [stage_rows][pitch], then one query row per warp
+  float* q = scan_smem + (size_t)a.stage_rows * ix.pitch + (size_t)warp * ix.pitch;
+  const int64_t qi = (int64_t)blockIdx.x * kScanWarps + warp;
+  const bool qvalid = qi < a.nq;
+  // the query in the permuted layout, normalised for cosine as the search normalises it
+  for (int e = lane; e < ix.pitch; e += 32) q[e] = 0.0f;
+  __syncwarp();
+  if (qvalid) {
+    const float* src = a.queries + qi * ix.dim;
+    float s = 1.0f;
+    bool scale = false;
+    if (ix.dist_type == kNormCosine) {
+      if (lane == 0) {
+        float sum = 0.0f;
+        for (int e = 0; e < ix.dim; ++e) sum = __fadd_rn(sum, __fmul_rn(src[e], src[e]));
+        if (sum != 0.0f) {
+          s = __fdiv_rn(1.0f, __fsqrt_rn(sum));
+          scale = true;
+        }
+      }
+      s = __shfl_sync(kFull, s, 0);
+      scale = __shfl_sync(kFull, scale, 0);
+    }
+    for (int e = lane; e < ix.dim; e += 32) {
+      float v = src[e];
+      if (scale) v = __fmul_rn(v, s);
+      q[permuted_pos(e, ix.dim)] = v;
+    }
+  }
+  __syncwarp();
+  const bool lp = ix.dist_type == kL1 || ix.dist_type == kLInf;
+  const int code = ix.dist_type;
+  const int nfull = ix.n16 >> 5;
+  const bool half = (ix.n16 & 31) != 0;
+  const int nf4 = (ix.dim + 3) >> 2;
+  float bd = INFINITY;
+  int bi = 0x7fffffff;
+  const int64_t r0 = (int64_t)blockIdx.y * a.chunk_rows, r1 = min(ix.n, r0 + a.chunk_rows);
+  for (int64_t base = r0; base < r1; base += a.stage_rows) {
+    const int cnt = (int)min((int64_t)a.stage_rows, r1 - base);
+    __syncthreads();  // every warp is done with the previous round's rows
+    for (int t = threadIdx.x; t < cnt * nf4; t += blockDim.x) {
+      const int r = t / nf4, c = t - r * nf4;
+      cp_async16(rows + (size_t)r * ix.pitch + 4 * c, ix.vecs + (base + r) * ix.pitch + 4 * c);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (!qvalid) continue;
+    for (int rr = 0; rr < cnt; rr += 4) {
+      const int r = rr + g;
+      const bool act = r < cnt;
+      const float* row = rows + (size_t)(act ? r : 0) * ix.pitch;
+      float d;
+      if (lp) {
+        d = lp_group_dist<false>(ix, q, row, act);
+      } else {
+        float acc = 0.0f;
+        for (int c = 0; c < nfull; ++c) {
+          const float4 qv = reinterpret_cast<const float4*>(q + c * 32)[j];
+          const float4 x = reinterpret_cast<const float4*>(row + c * 32)[j];
+          acc = fma_term(code, qv.x, x.x, acc);
+          acc = fma_term(code, qv.y, x.y, acc);
+          acc = fma_term(code, qv.z, x.z, acc);
+          acc = fma_term(code, qv.w, x.w, acc);
+        }
+        if (half) {
+          const float2 qv = reinterpret_cast<const float2*>(q + nfull * 32)[j];
+          const float2 x = reinterpret_cast<const float2*>(row + nfull * 32)[j];
+          acc = fma_term(code, qv.x, x.x, acc);
+          acc = fma_term(code, qv.y, x.y, acc);
+        }
+        d = combine(ix, acc, row, q);
+      }
+#pragma unroll
+      for (int gg = 0; gg < 4; ++gg) {
+        const float dc = __shfl_sync(kFull, d, gg * 8);
+        if (rr + gg < cnt) scan_offer(bd, bi, a.k, dc, (int)(base + rr + gg));
+      }
+    }
+  }
+  if (qvalid && lane < a.k) {
+    const size_t o = ((size_t)qi * a.n_chunks + blockIdx.y) * a.k + lane;
+    a.part_d[o] = bd;
+    a.part_id[o] = bi;
+  }
+}
+
+// One warp per query: the best k of its chunks' lists, then external ids.
+__global__ void scan_merge_kernel(const float* __restrict__ part_d, const int32_t* __restrict__ part_id, int64_t nq,
+                                  int n_chunks, int k, int kmax, const int32_t* __restrict__ ext_id,
+                                  int32_t* __restrict__ ids, float* __restrict__ dists, int32_t* __restrict__ counts) {
+  const int lane = lane_id();
+  const int64_t qi = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (qi >= nq) return;
+  float bd = INFINITY;
+  int bi = 0x7fffffff;
+  for (int c = 0; c < n_chunks; ++c) {
+    const size_t o = ((size_t)qi * n_chunks + c) * k;
+    for (int i = 0; i < k; ++i) {
+      const float d = part_d[o + i];
+      const int r = part_id[o + i];
+      if (r == 0x7fffffff) break;  // the chunk's list ends here
+      scan_offer(bd, bi, k, d, r);
+    }
+  }
+  const int have = __popc(__ballot_sync(kFull, lane < k && bi != 0x7fffffff));
+  for (int i = lane; i < kmax; i += 32) {
+    const bool ok = i < have;
+    ids[qi * kmax + i] = ok ? __ldg(ext_id + bi) : -1;
+    dists[qi * kmax + i] = ok ? bd : __int_as_float(0x7f800000);
+  }
+  if (lane == 0) counts[qi] = have;
+}
+
 }  // namespace
+
+int exact_scan_knn(const DevIndex& ix, const float* queries, int64_t nq, int k, int kmax, float* part_d,
+                   int32_t* part_id, int n_chunks, int32_t* ids, float* dists, int32_t* counts, void* stream) {
+  if (nq == 0) return 0;
+  if (k < 1 || k > 32) return (int)cudaErrorInvalidValue;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int row_bytes = ix.pitch * 4;
+  const int budget = 200 * 1024 - kScanWarps * row_bytes;
+  const int stage_rows = std::min(32, budget / row_bytes) & ~3;
+  if (stage_rows < 4) return (int)cudaErrorInvalidValue;
+  ScanArgs a;
+  a.ix = ix;
+  a.queries = queries;
+  a.nq = nq;
+  a.k = k;
+  a.n_chunks = n_chunks;
+  a.chunk_rows = (ix.n + n_chunks - 1) / n_chunks;
+  a.stage_rows = stage_rows;
+  a.part_d = part_d;
+  a.part_id = part_id;
+  const int smem = (stage_rows + kScanWarps) * row_bytes;
+  const int rc = allow_max_smem((const void*)exact_scan_kernel);
+  if (rc != 0) return rc;
+  cudaError_t e;
+  const dim3 grid((unsigned)((nq + kScanWarps - 1) / kScanWarps), (unsigned)n_chunks);
+  exact_scan_kernel<<<grid, 32 * kScanWarps, smem, st>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  scan_merge_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(part_d, part_id, nq, n_chunks, k, kmax, ix.ext_id, ids,
+                                                              dists, counts);
+  return (int)cudaGetLastError();
+}
 
 int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int hash_log2, int stage_rows) {
   int bytes = ix.pitch * 4 + region_items * 8 + nbpad * 16 + (hash_log2 > 0 ? (4 << hash_log2) : 0) +
@@ -1242,12 +1440,26 @@ Kern kernel_for(bool plain, int gather, bool with_old) {
 }
 }  // namespace
 
+int allow_max_smem(const void* kern) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, kern})) return 0;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
+  if (e != cudaSuccess) return (int)e;
+  done.insert({dev, kern});
+  return 0;
+}
+
 int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, int blocks, int warps_per_block,
                   void* stream) {
   Kern kern = kernel_for(plain, gather, with_old);
   const int smem = a.warp_smem * (plain ? 1 : warps_per_block);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return (int)e;
+  const int rc = allow_max_smem((const void*)kern);
+  if (rc != 0) return rc;
   if (plain)
     kern<<<(unsigned)a.nq, 32, smem, (cudaStream_t)stream>>>(a);
   else
@@ -1258,8 +1470,8 @@ int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, in
 int search_occupancy(bool plain, int gather, bool with_old, int warps_per_block, int smem_per_block,
                      int* blocks_per_sm) {
   Kern kern = kernel_for(plain, gather, with_old);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_per_block);
-  if (e != cudaSuccess) return (int)e;
+  const int rc = allow_max_smem((const void*)kern);
+  if (rc != 0) return rc;
   return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, 32 * (plain ? 1 : warps_per_block),
                                                             smem_per_block);
 }

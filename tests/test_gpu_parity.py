@@ -181,3 +181,37 @@ def test_cuda_graph_launch_matches():
             torch.cuda.synchronize()
             np.testing.assert_array_equal(ids.cpu().numpy(), want[0])
             np.testing.assert_array_equal(c.cpu().numpy(), want[2])
+
+
+def test_concurrent_launches_with_different_shared_memory():
+    """Two handles searched from two threads at once, with beams of very different sizes: the
+    same kernels launch concurrently with different shared-memory sizes, and neither launch may
+    be refused (the shared-memory limit is a process-wide property of each kernel)."""
+    import threading
+    q = np.ascontiguousarray(load_golden("c1_l2_d128")["queries"])
+    handles = []
+    for _ in range(2):
+        idx = nmslib.init(method="hnsw", space="l2")
+        idx.loadIndex(golden_path("c1_l2_d128"))
+        handles.append(idx)
+    want = []
+    for idx, (ef, k) in zip(handles, [(16, 5), (800, 100)]):
+        idx.setQueryTimeParams({"efSearch": ef})
+        want.append(idx.knnQueryBatchArrays(q, k)[0])
+    errors = []
+
+    def run(idx, k, ref):
+        try:
+            for _ in range(40):
+                ids = idx.knnQueryBatchArrays(q, k)[0]
+                np.testing.assert_array_equal(ids, ref)
+        except Exception as e:  # noqa: BLE001 - reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=run, args=(handles[0], 5, want[0])),
+               threading.Thread(target=run, args=(handles[1], 100, want[1]))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
