@@ -109,6 +109,20 @@ __device__ __forceinline__ int next_active_item(const GemmArgs& a, int item, int
   return item;
 }
 
+// v[i] for a lane-dependent i, by five levels of selects (no local memory).
+__device__ __forceinline__ float pick32(const float (&v)[32], int i) {
+  float a[16];
+#pragma unroll
+  for (int t = 0; t < 16; ++t) a[t] = (i & 16) ? v[t + 16] : v[t];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) a[t] = (i & 8) ? a[t + 8] : a[t];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) a[t] = (i & 4) ? a[t + 4] : a[t];
+#pragma unroll
+  for (int t = 0; t < 2; ++t) a[t] = (i & 2) ? a[t + 2] : a[t];
+  return (i & 1) ? a[1] : a[0];
+}
+
 // A row's candidate list is a min-heap of CAND (key, column) pairs in shared memory: the root is
 // the smallest kept key, i.e. the threshold a new key must beat. The first CAND offers fill it,
 // then it is heapified once; later insertions replace the root and sift down (log2 CAND steps).
@@ -375,17 +389,23 @@ __global__ void __launch_bounds__(kThreads, 1)
             // one warp vote first: the common case (no row of the warp passes) skips the
             // divergent region entirely
             if (__any_sync(0xffffffffu, mx >= thr)) {
-              if (mx >= thr) {
-                // plain stores into this row's own list: no atomics, nothing to wait for
+              // this row's hits as a bit mask built with selects (no branch per column), then one
+              // store pair per hit in a loop whose trip count is the warp's largest hit count
+              // (usually 1), the key taken out of the registers by a select tree: plain stores
+              // into the row's own list
+              unsigned hm = 0;
 #pragma unroll
-                for (int i = 0; i < 32; ++i)
-                  if (v[i] >= thr) {
-                    if (ncoll < a.list_len) {
-                      cid[ncoll] = col0 + i;
-                      ckey[ncoll] = v[i];
-                    }
-                    ++ncoll;
+              for (int i = 0; i < 32; ++i) hm |= (v[i] >= thr ? 1u : 0u) << i;
+              while (__any_sync(0xffffffffu, hm != 0)) {
+                if (hm) {
+                  const int i = __ffs(hm) - 1;
+                  hm &= hm - 1;
+                  if (ncoll < a.list_len) {
+                    cid[ncoll] = col0 + i;
+                    ckey[ncoll] = pick32(v, i);
                   }
+                  ++ncoll;
+                }
               }
             }
           }
