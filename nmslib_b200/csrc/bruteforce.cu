@@ -905,16 +905,18 @@ int scan_fallback(nmsg_index* h, const float* queries, int64_t nq, int dim, int 
   BruteForceState* s = h->bf ? h->bf : (h->bf = new BruteForceState());
   const DevIndex& d = h->dev;
   const int64_t q_blocks = (nq + 7) / 8;
+  // many small blocks (about 16 per SM) keep the last wave short
   const int n_chunks = (int)std::max<int64_t>(
-      1, std::min<int64_t>((4 * h->num_sms + q_blocks - 1) / q_blocks, std::max<int64_t>(1, d.n / 2048)));
+      1, std::min<int64_t>((16 * h->num_sms + q_blocks - 1) / q_blocks, std::max<int64_t>(1, d.n / 2048)));
+  const size_t n_part = (size_t)nq * n_chunks * exact_scan_lists(d) * k;
   const float* qin = queries;
   if (!dev_ptrs) {
     BF_CUDA(s->h_q.ensure((size_t)nq * dim * 4, false), "cudaMalloc(query staging)");
     BF_CUDA(cudaMemcpyAsync(s->h_q.p, queries, (size_t)nq * dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
     qin = s->h_q.as<float>();
   }
-  BF_CUDA(s->scr_key.ensure((size_t)nq * n_chunks * k * 4, false), "cudaMalloc(scan lists)");
-  BF_CUDA(s->scr_id.ensure((size_t)nq * n_chunks * k * 4, false), "cudaMalloc(scan lists)");
+  BF_CUDA(s->scr_key.ensure(n_part * 4, false), "cudaMalloc(scan lists)");
+  BF_CUDA(s->scr_id.ensure(n_part * 4, false), "cudaMalloc(scan lists)");
   int32_t* o_ids = ids;
   float* o_d = dists;
   int32_t* o_c = counts;

@@ -133,9 +133,11 @@ constexpr int kMaxDynamicSmem = 227 * 1024;
 // threads (serving lanes, concurrent callers) that need more. Returns a cudaError_t value.
 int allow_max_smem(const void* kern);
 // Exact k-NN (k <= 32) by scanning every row with the query path's distance arithmetic, on CUDA
-// cores (hnsw_search.cu): rows split into n_chunks per query block; part_d / part_id are
-// [nq][n_chunks][k] scratch. Outputs as the search writes them (external ids, -1 / +inf padding).
-// Returns a cudaError_t value.
+// cores (hnsw_search.cu): rows split into n_chunks per query block, each chunk kept as
+// exact_scan_lists(ix) partial lists; part_d / part_id are [nq][n_chunks * exact_scan_lists(ix)][k]
+// scratch. Outputs as the search writes them (external ids, -1 / +inf padding). Returns a
+// cudaError_t value.
+int exact_scan_lists(const DevIndex& ix);
 int exact_scan_knn(const DevIndex& ix, const float* queries, int64_t nq, int k, int kmax, float* part_d,
                    int32_t* part_id, int n_chunks, int32_t* ids, float* dists, int32_t* counts, void* stream);
 

@@ -1213,7 +1213,8 @@ __global__ void __launch_bounds__(32, 32) search_plain_kernel(SearchArgs a) {
 
 // ------------------------------------------------------------------ exact scan on CUDA cores
 // Exact k-NN (SeqSearch semantics, similarity_search/src/method/seqsearch.cc:143-177) for what the
-// tensor-core brute force does not take: L1 / LInf and rows wider than 256. A block of kScanWarps
+// tensor-core brute force does not take: L1 / LInf and rows wider than 256 (the fused-multiply-add
+// codes take exact_scan_tiled_kernel below; this kernel serves L1 / LInf). A block of kScanWarps
 // warps owns kScanWarps queries and one chunk of base rows; the rows are staged into shared memory
 // a round at a time and every warp computes its query's distances with the query path's own
 // arithmetic (so each distance is the value the HNSW search reports), keeping its best k by
@@ -1242,31 +1243,15 @@ __device__ __forceinline__ void scan_offer(float& bd, int& bi, int k, float d, i
   }
 }
 
-struct ScanArgs {
-  DevIndex ix;
-  const float* queries;  // [nq][dim]
-  int64_t nq;
-  int k;                 // <= 32
-  int64_t chunk_rows;
-  int n_chunks;
-  int stage_rows;        // rows per staged round (multiple of 4)
-  float* part_d;         // [nq][n_chunks][k]
-  int32_t* part_id;
-};
-
-__global__ void __launch_bounds__(32 * kScanWarps) exact_scan_kernel(ScanArgs a) {
-  extern __shared__ __align__(16) float scan_smem[];
-  const DevIndex& ix = a.ix;
-  const int warp = threadIdx.x >> 5, lane = lane_id(), g = lane >> 3, j = lane & 7;
-  float* rows = scan_smem;  // [stage_rows][pitch], then one query row per warp
-  float* q = scan_smem + (size_t)a.stage_rows * ix.pitch + (size_t)warp * ix.pitch;
-  const int64_t qi = (int64_t)blockIdx.x * kScanWarps + warp;
-  const bool qvalid = qi < a.nq;
-  // the query in the permuted layout, normalised for cosine as the search normalises it
+// One warp writes query qi (zeros when !valid) into q[pitch] in the permuted layout, normalised
+// for cosine as the search normalises it.
+__device__ void scan_load_query(const DevIndex& ix, const float* __restrict__ queries, int64_t qi, bool valid,
+                                float* q) {
+  const int lane = lane_id();
   for (int e = lane; e < ix.pitch; e += 32) q[e] = 0.0f;
   __syncwarp();
-  if (qvalid) {
-    const float* src = a.queries + qi * ix.dim;
+  if (valid) {
+    const float* src = queries + qi * ix.dim;
     float s = 1.0f;
     bool scale = false;
     if (ix.dist_type == kNormCosine) {
@@ -1288,6 +1273,29 @@ __global__ void __launch_bounds__(32 * kScanWarps) exact_scan_kernel(ScanArgs a)
     }
   }
   __syncwarp();
+}
+
+struct ScanArgs {
+  DevIndex ix;
+  const float* queries;  // [nq][dim]
+  int64_t nq;
+  int k;                 // <= 32
+  int64_t chunk_rows;
+  int n_chunks;
+  int stage_rows;        // rows per staged round (multiple of 4)
+  float* part_d;         // [nq][n_chunks][k]
+  int32_t* part_id;
+};
+
+__global__ void __launch_bounds__(32 * kScanWarps) exact_scan_kernel(ScanArgs a) {
+  extern __shared__ __align__(16) float scan_smem[];
+  const DevIndex& ix = a.ix;
+  const int warp = threadIdx.x >> 5, lane = lane_id(), g = lane >> 3, j = lane & 7;
+  float* rows = scan_smem;  // [stage_rows][pitch], then one query row per warp
+  float* q = scan_smem + (size_t)a.stage_rows * ix.pitch + (size_t)warp * ix.pitch;
+  const int64_t qi = (int64_t)blockIdx.x * kScanWarps + warp;
+  const bool qvalid = qi < a.nq;
+  scan_load_query(ix, a.queries, qi, qvalid, q);
   const bool lp = ix.dist_type == kL1 || ix.dist_type == kLInf;
   const int code = ix.dist_type;
   const int nfull = ix.n16 >> 5;
@@ -1345,6 +1353,135 @@ __global__ void __launch_bounds__(32 * kScanWarps) exact_scan_kernel(ScanArgs a)
   }
 }
 
+// The same scan for the fused-multiply-add codes (squared L2, cosine, negative dot), register
+// tiled: a block holds kTileQ queries in shared memory and its warps split the chunk's rows, each
+// 8-lane group taking kTileR rows at a time straight from global memory. Lane j of a group keeps
+// one accumulator per (row, query) pair and adds the same elements in the same order as the
+// search's lane j (elements 4j..4j+3 of every 32-element block, then 2j..2j+1 of the 16-element
+// block), and combine() finishes each pair as the search does, so every distance is the search's
+// value bit for bit. A pass costs 8 shared-memory and 4 global 16-byte loads per 128 FMAs, against
+// 2 loads per 4 FMAs when a warp owns one query. Each warp keeps its own best-k list per query.
+constexpr int kTileQ = 8;
+constexpr int kTileR = 4;
+constexpr int kTileWarps = 8;
+static_assert(kTileQ == kTileWarps, "one warp loads each query");
+
+template <bool kSub>
+__device__ __forceinline__ float tile_term(float a, float b, float acc) {
+  if constexpr (kSub) {
+    const float d = __fsub_rn(a, b);
+    return __fmaf_rn(d, d, acc);
+  } else {
+    return __fmaf_rn(a, b, acc);
+  }
+}
+
+template <bool kSub>
+__global__ void __launch_bounds__(32 * kTileWarps, 2) exact_scan_tiled_kernel(ScanArgs a) {
+  extern __shared__ __align__(16) float scan_smem[];
+  const DevIndex& ix = a.ix;
+  const int warp = threadIdx.x >> 5, lane = lane_id(), g = lane >> 3, j = lane & 7;
+  const int64_t q0 = (int64_t)blockIdx.x * kTileQ;
+  const int nq_here = (int)min((int64_t)kTileQ, a.nq - q0);
+  scan_load_query(ix, a.queries, q0 + warp, warp < nq_here, scan_smem + (size_t)warp * ix.pitch);
+  __syncthreads();
+  const float* qs = scan_smem;  // [kTileQ][pitch]
+  const int nfull = ix.n16 >> 5;
+  const bool half = (ix.n16 & 31) != 0;
+  float bd[kTileQ];
+  int bi[kTileQ];
+#pragma unroll
+  for (int qq = 0; qq < kTileQ; ++qq) {
+    bd[qq] = INFINITY;
+    bi[qq] = 0x7fffffff;
+  }
+  constexpr int kWarpRows = 4 * kTileR;  // rows a warp takes per pass
+  const int64_t r0 = (int64_t)blockIdx.y * a.chunk_rows, r1 = min(ix.n, r0 + a.chunk_rows);
+  for (int64_t wb = r0 + (int64_t)warp * kWarpRows; wb < r1; wb += (int64_t)kTileWarps * kWarpRows) {
+    // rows past the chunk's end read its last row and are never offered
+    const float* rp[kTileR];
+#pragma unroll
+    for (int r = 0; r < kTileR; ++r) rp[r] = ix.vecs + min(wb + g * kTileR + r, r1 - 1) * ix.pitch;
+    float acc[kTileR][kTileQ];
+#pragma unroll
+    for (int r = 0; r < kTileR; ++r)
+#pragma unroll
+      for (int qq = 0; qq < kTileQ; ++qq) acc[r][qq] = 0.0f;
+    float4 x[kTileR];
+    if (nfull > 0) {
+#pragma unroll
+      for (int r = 0; r < kTileR; ++r) x[r] = __ldg(reinterpret_cast<const float4*>(rp[r]) + j);
+    }
+    for (int c = 0; c < nfull; ++c) {
+      // next block's row values, loaded while this block's FMAs run (the last pass reloads it)
+      const int cn = min(c + 1, nfull - 1);
+      float4 xn[kTileR];
+#pragma unroll
+      for (int r = 0; r < kTileR; ++r) xn[r] = __ldg(reinterpret_cast<const float4*>(rp[r] + cn * 32) + j);
+#pragma unroll
+      for (int qq = 0; qq < kTileQ; ++qq) {
+        const float4 qv = reinterpret_cast<const float4*>(qs + (size_t)qq * ix.pitch + c * 32)[j];
+#pragma unroll
+        for (int r = 0; r < kTileR; ++r) {
+          acc[r][qq] = tile_term<kSub>(qv.x, x[r].x, acc[r][qq]);
+          acc[r][qq] = tile_term<kSub>(qv.y, x[r].y, acc[r][qq]);
+          acc[r][qq] = tile_term<kSub>(qv.z, x[r].z, acc[r][qq]);
+          acc[r][qq] = tile_term<kSub>(qv.w, x[r].w, acc[r][qq]);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kTileR; ++r) x[r] = xn[r];
+    }
+    if (half) {
+      float2 xv[kTileR];
+#pragma unroll
+      for (int r = 0; r < kTileR; ++r) xv[r] = __ldg(reinterpret_cast<const float2*>(rp[r] + nfull * 32) + j);
+#pragma unroll
+      for (int qq = 0; qq < kTileQ; ++qq) {
+        const float2 qv = reinterpret_cast<const float2*>(qs + (size_t)qq * ix.pitch + nfull * 32)[j];
+#pragma unroll
+        for (int r = 0; r < kTileR; ++r) {
+          acc[r][qq] = tile_term<kSub>(qv.x, xv[r].x, acc[r][qq]);
+          acc[r][qq] = tile_term<kSub>(qv.y, xv[r].y, acc[r][qq]);
+        }
+      }
+    }
+    // finish each pair, then offer the group leaders' distances that beat the query's k-th
+#pragma unroll
+    for (int qq = 0; qq < kTileQ; ++qq) {
+      float dv[kTileR];
+#pragma unroll
+      for (int r = 0; r < kTileR; ++r) dv[r] = combine(ix, acc[r][qq], rp[r], qs + (size_t)qq * ix.pitch);
+      if (qq >= nq_here) continue;
+#pragma unroll
+      for (int r = 0; r < kTileR; ++r) {
+        const int row = (int)(wb + g * kTileR + r);
+        const float kd = __shfl_sync(kFull, bd[qq], a.k - 1);
+        const int ki = __shfl_sync(kFull, bi[qq], a.k - 1);
+        unsigned m = __ballot_sync(kFull, j == 0 && wb + g * kTileR + r < r1 && scan_better(dv[r], row, kd, ki));
+        while (m) {
+          const int src = __ffs(m) - 1;
+          m &= m - 1;
+          const float dc = __shfl_sync(kFull, dv[r], src);
+          const int rc = __shfl_sync(kFull, row, src);
+          scan_offer(bd[qq], bi[qq], a.k, dc, rc);
+        }
+      }
+    }
+  }
+  if (lane < a.k) {
+    const int n_lists = a.n_chunks * kTileWarps;
+#pragma unroll
+    for (int qq = 0; qq < kTileQ; ++qq) {
+      if (qq < nq_here) {
+        const size_t o = ((size_t)(q0 + qq) * n_lists + (size_t)blockIdx.y * kTileWarps + warp) * a.k + lane;
+        a.part_d[o] = bd[qq];
+        a.part_id[o] = bi[qq];
+      }
+    }
+  }
+}
+
 // One warp per query: the best k of its chunks' lists, then external ids.
 __global__ void scan_merge_kernel(const float* __restrict__ part_d, const int32_t* __restrict__ part_id, int64_t nq,
                                   int n_chunks, int k, int kmax, const int32_t* __restrict__ ext_id,
@@ -1374,15 +1511,19 @@ __global__ void scan_merge_kernel(const float* __restrict__ part_d, const int32_
 
 }  // namespace
 
+static bool scan_tiled(const DevIndex& ix) {
+  return ix.dist_type == kL2Sqr16Ext || ix.dist_type == kL2SqrExt || ix.dist_type == kNormCosine ||
+         ix.dist_type == kNegDot;
+}
+
+int exact_scan_lists(const DevIndex& ix) { return scan_tiled(ix) ? kTileWarps : 1; }
+
 int exact_scan_knn(const DevIndex& ix, const float* queries, int64_t nq, int k, int kmax, float* part_d,
                    int32_t* part_id, int n_chunks, int32_t* ids, float* dists, int32_t* counts, void* stream) {
   if (nq == 0) return 0;
   if (k < 1 || k > 32) return (int)cudaErrorInvalidValue;
   cudaStream_t st = (cudaStream_t)stream;
   const int row_bytes = ix.pitch * 4;
-  const int budget = 200 * 1024 - kScanWarps * row_bytes;
-  const int stage_rows = std::min(32, budget / row_bytes) & ~3;
-  if (stage_rows < 4) return (int)cudaErrorInvalidValue;
   ScanArgs a;
   a.ix = ix;
   a.queries = queries;
@@ -1390,19 +1531,39 @@ int exact_scan_knn(const DevIndex& ix, const float* queries, int64_t nq, int k, 
   a.k = k;
   a.n_chunks = n_chunks;
   a.chunk_rows = (ix.n + n_chunks - 1) / n_chunks;
-  a.stage_rows = stage_rows;
   a.part_d = part_d;
   a.part_id = part_id;
-  const int smem = (stage_rows + kScanWarps) * row_bytes;
-  const int rc = allow_max_smem((const void*)exact_scan_kernel);
-  if (rc != 0) return rc;
   cudaError_t e;
-  const dim3 grid((unsigned)((nq + kScanWarps - 1) / kScanWarps), (unsigned)n_chunks);
-  exact_scan_kernel<<<grid, 32 * kScanWarps, smem, st>>>(a);
+  if (scan_tiled(ix)) {
+    a.stage_rows = 0;
+    const int smem = kTileQ * row_bytes;
+    if (smem > kMaxDynamicSmem) return (int)cudaErrorInvalidValue;
+    const bool sub = ix.dist_type == kL2Sqr16Ext || ix.dist_type == kL2SqrExt;
+    const void* kern = sub ? (const void*)exact_scan_tiled_kernel<true> : (const void*)exact_scan_tiled_kernel<false>;
+    const int rc = allow_max_smem(kern);
+    if (rc != 0) return rc;
+    const dim3 grid((unsigned)((nq + kTileQ - 1) / kTileQ), (unsigned)n_chunks);
+    if (sub)
+      exact_scan_tiled_kernel<true><<<grid, 32 * kTileWarps, smem, st>>>(a);
+    else
+      exact_scan_tiled_kernel<false><<<grid, 32 * kTileWarps, smem, st>>>(a);
+  } else {
+    // stage at most 32 rows within ~72 KB per block (three blocks per SM even for wide rows:
+    // the loop is latency-bound and needs the warps), at least 4 rows when the rows are wider
+    const int stage_rows =
+        std::max(std::min(32, (72 * 1024 - kScanWarps * row_bytes) / row_bytes) & ~3, 4);
+    if ((stage_rows + kScanWarps) * row_bytes > kMaxDynamicSmem) return (int)cudaErrorInvalidValue;
+    a.stage_rows = stage_rows;
+    const int smem = (stage_rows + kScanWarps) * row_bytes;
+    const int rc = allow_max_smem((const void*)exact_scan_kernel);
+    if (rc != 0) return rc;
+    const dim3 grid((unsigned)((nq + kScanWarps - 1) / kScanWarps), (unsigned)n_chunks);
+    exact_scan_kernel<<<grid, 32 * kScanWarps, smem, st>>>(a);
+  }
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
-  scan_merge_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(part_d, part_id, nq, n_chunks, k, kmax, ix.ext_id, ids,
-                                                              dists, counts);
+  scan_merge_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(part_d, part_id, nq, n_chunks * exact_scan_lists(ix), k,
+                                                              kmax, ix.ext_id, ids, dists, counts);
   return (int)cudaGetLastError();
 }
 

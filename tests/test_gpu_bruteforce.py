@@ -82,6 +82,35 @@ def test_exact_scan_matches_reference_distances(name, k, nq):
     assert st[0] == 0 and st[1] == n and st[2] == 0
 
 
+@pytest.mark.parametrize("space,code,dim", [("l2", 0, 307), ("l2", 0, 320), ("cosinesimil", 1, 304),
+                                            ("negdotprod", 2, 271)])
+def test_exact_scan_wide_rows_tiled(tmp_path, space, code, dim):
+    """Rows wider than 256 in the fused-multiply-add spaces take the register-tiled scan: odd widths
+    (16-element half block, 4-wide and scalar tails), a row count that ends inside a warp's pass,
+    several chunks and a last query block of 4; every id and distance equals the oracle's full
+    scan bit for bit."""
+    rng = np.random.default_rng(dim)
+    n, nq, k = 4_333, 20, 12
+    base = rng.standard_normal((n, dim)).astype(np.float32)
+    q = rng.standard_normal((nq, dim)).astype(np.float32)
+    p = str(tmp_path / f"wide_{space}_{dim}.hnsw")
+    _capi.build_index(base, code, 4, 16, nthreads=0, out_path=p)
+    idx = nmslib.init(method="hnsw", space=space)
+    idx.loadIndex(p)
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True)
+    assert st[0] == 0 and st[1] == n and st[3] >= 2
+    ix = OracleIndex(p)
+    vecs, ext, _, _ = ix.export()
+    dt = ix.info["dist_type"]
+    for qi in range(nq):
+        qv = normalize(q[qi]) if space == "cosinesimil" else q[qi]
+        dd = np.array([dist(dt, qv, vecs[r]) for r in range(n)], np.float32)
+        order = np.lexsort((np.arange(n), dd))[:k]
+        assert cnt[qi] == k
+        np.testing.assert_array_equal(ids[qi], ext[order])
+        np.testing.assert_array_equal(d[qi], dd[order])
+
+
 def test_bruteforce_limits():
     idx = _index("c1_l2_d128")
     with pytest.raises(RuntimeError, match="k <= 32"):
