@@ -1360,11 +1360,14 @@ __global__ void __launch_bounds__(32 * kScanWarps) exact_scan_kernel(ScanArgs a)
 // search's lane j (elements 4j..4j+3 of every 32-element block, then 2j..2j+1 of the 16-element
 // block), and combine() finishes each pair as the search does, so every distance is the search's
 // value bit for bit. A pass costs 8 shared-memory and 4 global 16-byte loads per 128 FMAs, against
-// 2 loads per 4 FMAs when a warp owns one query. Each warp keeps its own best-k list per query.
+// 2 loads per 4 FMAs when a warp owns one query. Each warp keeps its own best-k list per query in
+// shared memory (offers are rare once the list fills; the k-th sits in a register).
 constexpr int kTileQ = 8;
 constexpr int kTileR = 4;
 constexpr int kTileWarps = 8;
 static_assert(kTileQ == kTileWarps, "one warp loads each query");
+static_assert(kTileQ <= 32, "one lane holds each query's k-th");
+constexpr int kTileWarpSmem = (kTileR * kTileQ + 2 * kTileQ) * 32;  // floats per warp
 
 template <bool kSub>
 __device__ __forceinline__ float tile_term(float a, float b, float acc) {
@@ -1386,15 +1389,19 @@ __global__ void __launch_bounds__(32 * kTileWarps, 2) exact_scan_tiled_kernel(Sc
   scan_load_query(ix, a.queries, q0 + warp, warp < nq_here, scan_smem + (size_t)warp * ix.pitch);
   __syncthreads();
   const float* qs = scan_smem;  // [kTileQ][pitch]
+  // per warp: the pass's lane partials [kTileR * kTileQ][32], then its best-k lists [kTileQ][32]
+  float* part = scan_smem + (size_t)kTileQ * ix.pitch + (size_t)warp * kTileWarpSmem;
+  float* list_d = part + kTileR * kTileQ * 32;
+  int* list_i = reinterpret_cast<int*>(list_d + kTileQ * 32);
+  for (int i = lane; i < kTileQ * 32; i += 32) {
+    list_d[i] = INFINITY;
+    list_i[i] = 0x7fffffff;
+  }
+  // lane qq < kTileQ holds query qq's current k-th (distance, row)
+  float kth_d = INFINITY;
+  int kth_i = 0x7fffffff;
   const int nfull = ix.n16 >> 5;
   const bool half = (ix.n16 & 31) != 0;
-  float bd[kTileQ];
-  int bi[kTileQ];
-#pragma unroll
-  for (int qq = 0; qq < kTileQ; ++qq) {
-    bd[qq] = INFINITY;
-    bi[qq] = 0x7fffffff;
-  }
   constexpr int kWarpRows = 4 * kTileR;  // rows a warp takes per pass
   const int64_t r0 = (int64_t)blockIdx.y * a.chunk_rows, r1 = min(ix.n, r0 + a.chunk_rows);
   for (int64_t wb = r0 + (int64_t)warp * kWarpRows; wb < r1; wb += (int64_t)kTileWarps * kWarpRows) {
@@ -1446,38 +1453,48 @@ __global__ void __launch_bounds__(32 * kTileWarps, 2) exact_scan_tiled_kernel(Sc
         }
       }
     }
-    // finish each pair, then offer the group leaders' distances that beat the query's k-th
+    // park the partials, then finish one pair at a time (a rolled loop keeps the code small)
 #pragma unroll
-    for (int qq = 0; qq < kTileQ; ++qq) {
-      float dv[kTileR];
+    for (int r = 0; r < kTileR; ++r)
 #pragma unroll
-      for (int r = 0; r < kTileR; ++r) dv[r] = combine(ix, acc[r][qq], rp[r], qs + (size_t)qq * ix.pitch);
+      for (int qq = 0; qq < kTileQ; ++qq) part[(r * kTileQ + qq) * 32 + lane] = acc[r][qq];
+    __syncwarp();
+    for (int p = 0; p < kTileR * kTileQ; ++p) {
+      const int r = p / kTileQ, qq = p - r * kTileQ;
+      const int64_t row = wb + g * kTileR + r;
+      const float d = combine(ix, part[p * 32 + lane], ix.vecs + min(row, r1 - 1) * ix.pitch, qs + (size_t)qq * ix.pitch);
       if (qq >= nq_here) continue;
-#pragma unroll
-      for (int r = 0; r < kTileR; ++r) {
-        const int row = (int)(wb + g * kTileR + r);
-        const float kd = __shfl_sync(kFull, bd[qq], a.k - 1);
-        const int ki = __shfl_sync(kFull, bi[qq], a.k - 1);
-        unsigned m = __ballot_sync(kFull, j == 0 && wb + g * kTileR + r < r1 && scan_better(dv[r], row, kd, ki));
+      const float kd = __shfl_sync(kFull, kth_d, qq);
+      const int ki = __shfl_sync(kFull, kth_i, qq);
+      unsigned m = __ballot_sync(kFull, j == 0 && row < r1 && scan_better(d, (int)row, kd, ki));
+      if (m) {
+        float bd = list_d[qq * 32 + lane];
+        int bi = list_i[qq * 32 + lane];
         while (m) {
           const int src = __ffs(m) - 1;
           m &= m - 1;
-          const float dc = __shfl_sync(kFull, dv[r], src);
-          const int rc = __shfl_sync(kFull, row, src);
-          scan_offer(bd[qq], bi[qq], a.k, dc, rc);
+          const float dc = __shfl_sync(kFull, d, src);
+          const int rc = __shfl_sync(kFull, (int)row, src);
+          scan_offer(bd, bi, a.k, dc, rc);
+        }
+        list_d[qq * 32 + lane] = bd;
+        list_i[qq * 32 + lane] = bi;
+        const float nd = __shfl_sync(kFull, bd, a.k - 1);
+        const int ni = __shfl_sync(kFull, bi, a.k - 1);
+        if (lane == qq) {
+          kth_d = nd;
+          kth_i = ni;
         }
       }
     }
+    __syncwarp();  // the next pass overwrites the partials
   }
   if (lane < a.k) {
     const int n_lists = a.n_chunks * kTileWarps;
-#pragma unroll
-    for (int qq = 0; qq < kTileQ; ++qq) {
-      if (qq < nq_here) {
-        const size_t o = ((size_t)(q0 + qq) * n_lists + (size_t)blockIdx.y * kTileWarps + warp) * a.k + lane;
-        a.part_d[o] = bd[qq];
-        a.part_id[o] = bi[qq];
-      }
+    for (int qq = 0; qq < nq_here; ++qq) {
+      const size_t o = ((size_t)(q0 + qq) * n_lists + (size_t)blockIdx.y * kTileWarps + warp) * a.k + lane;
+      a.part_d[o] = list_d[qq * 32 + lane];
+      a.part_id[o] = list_i[qq * 32 + lane];
     }
   }
 }
@@ -1536,7 +1553,7 @@ int exact_scan_knn(const DevIndex& ix, const float* queries, int64_t nq, int k, 
   cudaError_t e;
   if (scan_tiled(ix)) {
     a.stage_rows = 0;
-    const int smem = kTileQ * row_bytes;
+    const int smem = kTileQ * row_bytes + kTileWarps * kTileWarpSmem * 4;
     if (smem > kMaxDynamicSmem) return (int)cudaErrorInvalidValue;
     const bool sub = ix.dist_type == kL2Sqr16Ext || ix.dist_type == kL2SqrExt;
     const void* kern = sub ? (const void*)exact_scan_tiled_kernel<true> : (const void*)exact_scan_tiled_kernel<false>;
