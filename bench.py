@@ -306,6 +306,34 @@ def brute_force_measure(index, queries, k=10, reps=3):
     return res
 
 
+def profile_scan(n, calls, dim=960, nq=200):
+    """The exact CUDA-core scan (negdot rows wider than 256) through the public API, for ncu:
+    n x dim standard-normal rows and nq queries (seed 0), indexed by a small device-built graph
+    (M 4, efConstruction 8: the scan never reads it)."""
+    import torch
+    import nmslib_b200 as nmslib
+    from nmslib_b200 import _capi
+    from nmslib_b200.build import build
+    build()
+    rng = np.random.default_rng(0)
+    base = rng.standard_normal((n, dim), dtype=np.float32)
+    q = rng.standard_normal((nq, dim), dtype=np.float32)
+    os.makedirs(CACHE_DIR, exist_ok=True)
+    path = os.path.join(CACHE_DIR, f"scan_profile_{n}_{dim}.hnsw")
+    _capi.build_index(base, 2, 4, 8, nthreads=0, seed=0, out_path=path, device=0)
+    index = nmslib.init(method="hnsw", space="negdotprod")
+    index.loadIndex(path)
+    t = []
+    for _ in range(calls):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        index.bruteForceBatchArrays(q, K)
+        t.append(time.perf_counter() - t0)
+    best = min(t)
+    log(f"[bench] scan profile case: {calls} calls of {nq} queries over {n} x {dim}; best {best * 1e3:.2f} ms "
+        f"({2.0 * nq * n * dim / best / 1e12:.1f} TFLOP/s end to end)")
+
+
 def build_compare(base, space, m, queries, kth, host_recall, device):
     """The same index built with the level-0 construction searches on the GPU: wall time and
     recall@10 at the headline efSearch, beside the host build's."""
@@ -460,12 +488,18 @@ def main():
                     help="profiling run: only NQ queries at the headline efSearch, no sweep, no baselines")
     ap.add_argument("--profile-bruteforce", type=int, default=0, metavar="NQ",
                     help="profiling run: exact brute force (k=10) of NQ queries over the base, warmup + steps calls")
+    ap.add_argument("--profile-scan", type=int, default=0, metavar="N",
+                    help="profiling run: the exact CUDA-core scan alone (200 queries, k=10) over N x 960 normal "
+                         "rows (negdot, a small device-built graph), warmup + steps calls")
     ap.add_argument("--workload", choices=["c2", "c3", "c4", "c5"], default="c2",
                     help="c2 (default, the headline line); c3 cosine 1M x 100 + brute force; c4 negdot "
                          "1M x 960 mixed k/ef batch; c5 l2 5M x 96 serving")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.profile_scan:
+        profile_scan(args.profile_scan, args.warmup + args.steps)
+        return
     if args.workload != "c2":
         run_aux(args)
         return

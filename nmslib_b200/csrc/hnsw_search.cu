@@ -1499,22 +1499,39 @@ __global__ void __launch_bounds__(32 * kTileWarps, 2) exact_scan_tiled_kernel(Sc
   }
 }
 
-// One warp per query: the best k of its chunks' lists, then external ids.
+// One warp per query: the best k of its lists, then external ids. The query's lists are one run of
+// n_lists * k entries (a list's unused tail holds the (inf, 0x7fffffff) sentinel); the warp reads
+// 4 x 32 of them at a time, one per lane, and offers only those that beat its current k-th.
 __global__ void scan_merge_kernel(const float* __restrict__ part_d, const int32_t* __restrict__ part_id, int64_t nq,
-                                  int n_chunks, int k, int kmax, const int32_t* __restrict__ ext_id,
+                                  int n_lists, int k, int kmax, const int32_t* __restrict__ ext_id,
                                   int32_t* __restrict__ ids, float* __restrict__ dists, int32_t* __restrict__ counts) {
   const int lane = lane_id();
   const int64_t qi = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (qi >= nq) return;
   float bd = INFINITY;
   int bi = 0x7fffffff;
-  for (int c = 0; c < n_chunks; ++c) {
-    const size_t o = ((size_t)qi * n_chunks + c) * k;
-    for (int i = 0; i < k; ++i) {
-      const float d = part_d[o + i];
-      const int r = part_id[o + i];
-      if (r == 0x7fffffff) break;  // the chunk's list ends here
-      scan_offer(bd, bi, k, d, r);
+  const int total = n_lists * k;
+  const size_t base = (size_t)qi * total;
+  constexpr int kBatch = 4;
+  for (int t0 = 0; t0 < total; t0 += 32 * kBatch) {
+    float d[kBatch];
+    int r[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int t = t0 + u * 32 + lane;
+      d[u] = t < total ? __ldg(part_d + base + t) : INFINITY;
+      r[u] = t < total ? __ldg(part_id + base + t) : 0x7fffffff;
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const float kd = __shfl_sync(kFull, bd, k - 1);
+      const int ki = __shfl_sync(kFull, bi, k - 1);
+      unsigned m = __ballot_sync(kFull, r[u] != 0x7fffffff && scan_better(d[u], r[u], kd, ki));
+      while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        scan_offer(bd, bi, k, __shfl_sync(kFull, d[u], src), __shfl_sync(kFull, r[u], src));
+      }
     }
   }
   const int have = __popc(__ballot_sync(kFull, lane < k && bi != 0x7fffffff));
