@@ -111,6 +111,59 @@ def test_exact_scan_wide_rows_tiled(tmp_path, space, code, dim):
         np.testing.assert_array_equal(d[qi], dd[order])
 
 
+def _oracle_scan(p, q, k, cosine=False):
+    ix = OracleIndex(p)
+    vecs, ext, _, _ = ix.export()
+    dt = ix.info["dist_type"]
+    n = len(vecs)
+    out = []
+    for qi in range(len(q)):
+        qv = normalize(q[qi]) if cosine else q[qi]
+        dd = np.array([dist(dt, qv, vecs[r]) for r in range(n)], np.float32)
+        order = np.lexsort((np.arange(n), dd))[:k]
+        out.append((ext[order], dd[order]))
+    return out
+
+
+@pytest.mark.parametrize("k", [1, 32])
+def test_exact_scan_tiled_k_extremes_and_ties(tmp_path, k):
+    """4,333 rows that are copies of 37 distinct 288-wide vectors (every distance tied ~117 ways,
+    across warps, chunks and query blocks): the tiled scan and the list merge keep the lowest
+    rows of each tie, exactly as a full scan ordered by (distance, node) does."""
+    rng = np.random.default_rng(k)
+    distinct = rng.integers(-3, 4, (37, 288)).astype(np.float32)
+    base = distinct[rng.integers(0, 37, 4_333)]
+    q = np.concatenate([distinct[:5], rng.integers(-3, 4, (6, 288)).astype(np.float32)])
+    p = str(tmp_path / f"ties_{k}.hnsw")
+    _capi.build_index(base, 0, 4, 16, nthreads=0, out_path=p)
+    idx = nmslib.init(method="hnsw", space="l2")
+    idx.loadIndex(p)
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True)
+    assert st[0] == 0 and st[3] >= 2
+    for qi, (want_i, want_d) in enumerate(_oracle_scan(p, q, k)):
+        assert cnt[qi] == k
+        np.testing.assert_array_equal(ids[qi, :k], want_i)
+        np.testing.assert_array_equal(d[qi, :k], want_d)
+
+
+def test_exact_scan_tiled_zero_cosine_query(tmp_path):
+    """A zero query under cosine is not normalised (the search leaves it as is): every distance is
+    1 - 0 = 1 and the k lowest rows come back."""
+    rng = np.random.default_rng(3)
+    base = rng.standard_normal((3_000, 300)).astype(np.float32)
+    q = np.concatenate([np.zeros((1, 300), np.float32), rng.standard_normal((2, 300)).astype(np.float32)])
+    p = str(tmp_path / "zero_cos.hnsw")
+    _capi.build_index(base, 1, 4, 16, nthreads=0, out_path=p)
+    idx = nmslib.init(method="hnsw", space="cosinesimil")
+    idx.loadIndex(p)
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, 10, stats=True)
+    want = _oracle_scan(p, q, 10, cosine=True)
+    for qi, (want_i, want_d) in enumerate(want):
+        np.testing.assert_array_equal(ids[qi], want_i)
+        np.testing.assert_array_equal(d[qi], want_d)
+    np.testing.assert_array_equal(d[0], np.ones(10, np.float32))
+
+
 def test_bruteforce_limits():
     idx = _index("c1_l2_d128")
     with pytest.raises(RuntimeError, match="k <= 32"):
