@@ -257,6 +257,14 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
 }
 
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// waits until at most N of this thread's committed copy groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait_keep() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
@@ -1355,19 +1363,25 @@ __global__ void __launch_bounds__(32 * kScanWarps) exact_scan_kernel(ScanArgs a)
 
 // The same scan for the fused-multiply-add codes (squared L2, cosine, negative dot), register
 // tiled: a block holds kTileQ queries in shared memory and its warps split the chunk's rows, each
-// 8-lane group taking kTileR rows at a time straight from global memory. Lane j of a group keeps
+// 8-lane group taking kTileR rows at a time, streamed through a per-warp ring of asynchronous
+// 16-byte copies kTileStages blocks deep (each lane copies exactly the pieces it reads, so a lane
+// waits only for its own copies). Lane j of a group keeps
 // one accumulator per (row, query) pair and adds the same elements in the same order as the
 // search's lane j (elements 4j..4j+3 of every 32-element block, then 2j..2j+1 of the 16-element
 // block), and combine() finishes each pair as the search does, so every distance is the search's
-// value bit for bit. A pass costs 8 shared-memory and 4 global 16-byte loads per 128 FMAs, against
-// 2 loads per 4 FMAs when a warp owns one query. Each warp keeps its own best-k list per query in
+// value bit for bit. A pass costs 12 shared-memory 16-byte loads and 4 asynchronous copies per
+// 128 FMAs, against 2 loads per 4 FMAs when a warp owns one query. Each warp keeps its own best-k list per query in
 // shared memory (offers are rare once the list fills; the k-th sits in a register).
 constexpr int kTileQ = 8;
 constexpr int kTileR = 4;
 constexpr int kTileWarps = 8;
 static_assert(kTileQ == kTileWarps, "one warp loads each query");
 static_assert(kTileQ <= 32, "one lane holds each query's k-th");
-constexpr int kTileWarpSmem = (kTileR * kTileQ + 2 * kTileQ) * 32;  // floats per warp
+constexpr int kTileStages = 3;                       // blocks of rows in flight per warp
+constexpr int kTileStage = 4 * kTileR * 32;          // floats per stage: the warp's 16 rows x 32
+constexpr int kTileRing = kTileStages * kTileStage > kTileR * kTileQ * 32 ? kTileStages * kTileStage
+                                                                          : kTileR * kTileQ * 32;
+constexpr int kTileWarpSmem = kTileRing + 2 * kTileQ * 32;  // floats per warp
 
 template <bool kSub>
 __device__ __forceinline__ float tile_term(float a, float b, float acc) {
@@ -1389,9 +1403,10 @@ __global__ void __launch_bounds__(32 * kTileWarps, 2) exact_scan_tiled_kernel(Sc
   scan_load_query(ix, a.queries, q0 + warp, warp < nq_here, scan_smem + (size_t)warp * ix.pitch);
   __syncthreads();
   const float* qs = scan_smem;  // [kTileQ][pitch]
-  // per warp: the pass's lane partials [kTileR * kTileQ][32], then its best-k lists [kTileQ][32]
+  // per warp: the row ring [kTileStages][16 rows][32], which also holds the pass's parked lane
+  // partials [kTileR * kTileQ][32] once it has drained, then its best-k lists [kTileQ][32]
   float* part = scan_smem + (size_t)kTileQ * ix.pitch + (size_t)warp * kTileWarpSmem;
-  float* list_d = part + kTileR * kTileQ * 32;
+  float* list_d = part + kTileRing;
   int* list_i = reinterpret_cast<int*>(list_d + kTileQ * 32);
   for (int i = lane; i < kTileQ * 32; i += 32) {
     list_d[i] = INFINITY;
@@ -1414,17 +1429,30 @@ __global__ void __launch_bounds__(32 * kTileWarps, 2) exact_scan_tiled_kernel(Sc
     for (int r = 0; r < kTileR; ++r)
 #pragma unroll
       for (int qq = 0; qq < kTileQ; ++qq) acc[r][qq] = 0.0f;
-    float4 x[kTileR];
-    if (nfull > 0) {
+    // a ring of kTileStages 32-element blocks of the lane's own 4 rows (the ring shares its space
+    // with the parked partials; each lane reads only what its own copies wrote)
+    float* ring = part + (g * kTileR) * 32 + 4 * j;
 #pragma unroll
-      for (int r = 0; r < kTileR; ++r) x[r] = __ldg(reinterpret_cast<const float4*>(rp[r]) + j);
+    for (int sb = 0; sb < kTileStages - 1; ++sb) {
+      if (sb < nfull) {
+#pragma unroll
+        for (int r = 0; r < kTileR; ++r) cp_async16(ring + sb * kTileStage + r * 32, rp[r] + sb * 32 + 4 * j);
+      }
+      cp_async_commit();
     }
     for (int c = 0; c < nfull; ++c) {
-      // next block's row values, loaded while this block's FMAs run (the last pass reloads it)
-      const int cn = min(c + 1, nfull - 1);
-      float4 xn[kTileR];
+      const int cb = c + kTileStages - 1;
+      if (cb < nfull) {
+        const int slot = cb % kTileStages;
 #pragma unroll
-      for (int r = 0; r < kTileR; ++r) xn[r] = __ldg(reinterpret_cast<const float4*>(rp[r] + cn * 32) + j);
+        for (int r = 0; r < kTileR; ++r) cp_async16(ring + slot * kTileStage + r * 32, rp[r] + cb * 32 + 4 * j);
+      }
+      cp_async_commit();
+      cp_async_wait_keep<kTileStages - 1>();
+      const float* src = ring + (c % kTileStages) * kTileStage;
+      float4 x[kTileR];
+#pragma unroll
+      for (int r = 0; r < kTileR; ++r) x[r] = *reinterpret_cast<const float4*>(src + r * 32);
 #pragma unroll
       for (int qq = 0; qq < kTileQ; ++qq) {
         const float4 qv = reinterpret_cast<const float4*>(qs + (size_t)qq * ix.pitch + c * 32)[j];
@@ -1436,9 +1464,9 @@ __global__ void __launch_bounds__(32 * kTileWarps, 2) exact_scan_tiled_kernel(Sc
           acc[r][qq] = tile_term<kSub>(qv.w, x[r].w, acc[r][qq]);
         }
       }
-#pragma unroll
-      for (int r = 0; r < kTileR; ++r) x[r] = xn[r];
     }
+    cp_async_wait_keep<0>();
+    __syncwarp();  // every lane is done with the ring before the partials are parked over it
     if (half) {
       float2 xv[kTileR];
 #pragma unroll
