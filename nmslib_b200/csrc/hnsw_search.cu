@@ -1221,13 +1221,10 @@ __global__ void __launch_bounds__(32, 32) search_plain_kernel(SearchArgs a) {
 
 // ------------------------------------------------------------------ exact scan on CUDA cores
 // Exact k-NN (SeqSearch semantics, similarity_search/src/method/seqsearch.cc:143-177) for what the
-// tensor-core brute force does not take: L1 / LInf and rows wider than 256 (the fused-multiply-add
-// codes take exact_scan_tiled_kernel below; this kernel serves L1 / LInf). A block of kScanWarps
-// warps owns kScanWarps queries and one chunk of base rows; the rows are staged into shared memory
-// a round at a time and every warp computes its query's distances with the query path's own
-// arithmetic (so each distance is the value the HNSW search reports), keeping its best k by
-// (distance, row) in a lane-distributed sorted list. scan_merge_kernel merges the chunks.
-constexpr int kScanWarps = 8;
+// tensor-core brute force does not take: L1 / LInf and rows wider than 256. A block owns kTileQ
+// queries and one chunk of base rows; every distance is computed with the query path's own
+// arithmetic (so it is the value the HNSW search reports), each warp keeps a best-k list by
+// (distance, row) per query, and scan_merge_kernel merges the lists.
 
 __device__ __forceinline__ bool scan_better(float da, int ia, float db, int ib) {
   return da < db || (da == db && ia < ib);
@@ -1290,79 +1287,11 @@ struct ScanArgs {
   int k;                 // <= 32
   int64_t chunk_rows;
   int n_chunks;
-  int stage_rows;        // rows per staged round (multiple of 4)
-  float* part_d;         // [nq][n_chunks][k]
+  float* part_d;         // [nq][n_chunks * kTileWarps][k]
   int32_t* part_id;
 };
 
-__global__ void __launch_bounds__(32 * kScanWarps) exact_scan_kernel(ScanArgs a) {
-  extern __shared__ __align__(16) float scan_smem[];
-  const DevIndex& ix = a.ix;
-  const int warp = threadIdx.x >> 5, lane = lane_id(), g = lane >> 3, j = lane & 7;
-  float* rows = scan_smem;  // [stage_rows][pitch], then one query row per warp
-  float* q = scan_smem + (size_t)a.stage_rows * ix.pitch + (size_t)warp * ix.pitch;
-  const int64_t qi = (int64_t)blockIdx.x * kScanWarps + warp;
-  const bool qvalid = qi < a.nq;
-  scan_load_query(ix, a.queries, qi, qvalid, q);
-  const bool lp = ix.dist_type == kL1 || ix.dist_type == kLInf;
-  const int code = ix.dist_type;
-  const int nfull = ix.n16 >> 5;
-  const bool half = (ix.n16 & 31) != 0;
-  const int nf4 = (ix.dim + 3) >> 2;
-  float bd = INFINITY;
-  int bi = 0x7fffffff;
-  const int64_t r0 = (int64_t)blockIdx.y * a.chunk_rows, r1 = min(ix.n, r0 + a.chunk_rows);
-  for (int64_t base = r0; base < r1; base += a.stage_rows) {
-    const int cnt = (int)min((int64_t)a.stage_rows, r1 - base);
-    __syncthreads();  // every warp is done with the previous round's rows
-    for (int t = threadIdx.x; t < cnt * nf4; t += blockDim.x) {
-      const int r = t / nf4, c = t - r * nf4;
-      cp_async16(rows + (size_t)r * ix.pitch + 4 * c, ix.vecs + (base + r) * ix.pitch + 4 * c);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    if (!qvalid) continue;
-    for (int rr = 0; rr < cnt; rr += 4) {
-      const int r = rr + g;
-      const bool act = r < cnt;
-      const float* row = rows + (size_t)(act ? r : 0) * ix.pitch;
-      float d;
-      if (lp) {
-        d = lp_group_dist<false>(ix, q, row, act);
-      } else {
-        float acc = 0.0f;
-        for (int c = 0; c < nfull; ++c) {
-          const float4 qv = reinterpret_cast<const float4*>(q + c * 32)[j];
-          const float4 x = reinterpret_cast<const float4*>(row + c * 32)[j];
-          acc = fma_term(code, qv.x, x.x, acc);
-          acc = fma_term(code, qv.y, x.y, acc);
-          acc = fma_term(code, qv.z, x.z, acc);
-          acc = fma_term(code, qv.w, x.w, acc);
-        }
-        if (half) {
-          const float2 qv = reinterpret_cast<const float2*>(q + nfull * 32)[j];
-          const float2 x = reinterpret_cast<const float2*>(row + nfull * 32)[j];
-          acc = fma_term(code, qv.x, x.x, acc);
-          acc = fma_term(code, qv.y, x.y, acc);
-        }
-        d = combine(ix, acc, row, q);
-      }
-#pragma unroll
-      for (int gg = 0; gg < 4; ++gg) {
-        const float dc = __shfl_sync(kFull, d, gg * 8);
-        if (rr + gg < cnt) scan_offer(bd, bi, a.k, dc, (int)(base + rr + gg));
-      }
-    }
-  }
-  if (qvalid && lane < a.k) {
-    const size_t o = ((size_t)qi * a.n_chunks + blockIdx.y) * a.k + lane;
-    a.part_d[o] = bd;
-    a.part_id[o] = bi;
-  }
-}
-
-// The same scan for the fused-multiply-add codes (squared L2, cosine, negative dot), register
-// tiled: a block holds kTileQ queries in shared memory and its warps split the chunk's rows, each
+// The fused-multiply-add codes (squared L2, cosine, negative dot), register tiled: a block holds kTileQ queries in shared memory and its warps split the chunk's rows, each
 // 8-lane group taking kTileR rows at a time, streamed through a per-warp ring of asynchronous
 // 16-byte copies kTileStages blocks deep (each lane copies exactly the pieces it reads, so a lane
 // waits only for its own copies). Lane j of a group keeps
@@ -1527,6 +1456,199 @@ __global__ void __launch_bounds__(32 * kTileWarps, 2) exact_scan_tiled_kernel(Sc
   }
 }
 
+// L1 / LInf, tiled the same way with 4-lane groups (8 per warp, kLpR rows each per pass). The
+// reference's L1 keeps four float accumulators, accumulator a adding |q_e - x_e| over
+// e == a (mod 4) in element order (distcomp_lp.cc:191-251). In the permuted layout the 16-byte
+// piece at position a of a 32-element block holds elements a, a+8, a+16, a+24 and the piece at
+// position a+4 holds a+4, a+12, a+20, a+28, so lane a of a group reads both (for the query and
+// its rows) and adds in exactly that order: the same accumulators as lp_group_dist, without its
+// shuffles. LInf is a maximum of non-negative values, which any order gives.
+constexpr int kLpR = 2;
+
+template <bool kL1>
+__device__ __forceinline__ float lp_term(float s, float q, float x) {
+  const float d = fabsf(__fsub_rn(q, x));
+  if constexpr (kL1) {
+    return __fadd_rn(s, d);
+  } else {
+    return fmaxf(s, d);
+  }
+}
+
+// Finishes one (row, query) pair from the 4 lane accumulators of each 4-lane group: the tails
+// past the 16-element blocks and the reference's final reduction. Every lane of the warp calls it.
+template <bool kL1>
+__device__ float lp_finish4(const DevIndex& ix, float s, const float* __restrict__ row, const float* __restrict__ q) {
+  const int lane = lane_id();
+  const int gb = lane & ~3, ac = lane & 3;
+  if constexpr (kL1) {
+    const int n4 = (ix.dim >> 2) << 2;
+    for (int e = ix.n16 + ac; e < n4; e += 4) s = __fadd_rn(s, fabsf(__fsub_rn(q[e], __ldg(row + e))));
+    float t = __fadd_rn(__shfl_sync(kFull, s, gb), __shfl_sync(kFull, s, gb + 1));
+    t = __fadd_rn(t, __shfl_sync(kFull, s, gb + 2));
+    t = __fadd_rn(t, __shfl_sync(kFull, s, gb + 3));
+    double r = (double)t;
+    for (int e = n4; e < ix.dim; ++e) r = __dadd_rn(r, (double)fabsf(__fsub_rn(q[e], __ldg(row + e))));
+    return __double2float_rn(r);
+  } else {
+    for (int e = ix.n16 + ac; e < ix.dim; e += 4) s = fmaxf(s, fabsf(__fsub_rn(q[e], __ldg(row + e))));
+    s = fmaxf(s, __shfl_xor_sync(kFull, s, 2, 4));
+    s = fmaxf(s, __shfl_xor_sync(kFull, s, 1, 4));
+    return s;
+  }
+}
+
+template <bool kL1>
+__global__ void __launch_bounds__(32 * kTileWarps, 2) exact_scan_lp_tiled_kernel(ScanArgs a) {
+  extern __shared__ __align__(16) float scan_smem[];
+  const DevIndex& ix = a.ix;
+  const int warp = threadIdx.x >> 5, lane = lane_id(), G = lane >> 2, ac = lane & 3;
+  const int64_t q0 = (int64_t)blockIdx.x * kTileQ;
+  const int nq_here = (int)min((int64_t)kTileQ, a.nq - q0);
+  scan_load_query(ix, a.queries, q0 + warp, warp < nq_here, scan_smem + (size_t)warp * ix.pitch);
+  __syncthreads();
+  const float* qs = scan_smem;  // [kTileQ][pitch]
+  // per warp: the row ring (which also holds the parked partials once drained), then the lists
+  float* part = scan_smem + (size_t)kTileQ * ix.pitch + (size_t)warp * kTileWarpSmem;
+  float* list_d = part + kTileRing;
+  int* list_i = reinterpret_cast<int*>(list_d + kTileQ * 32);
+  for (int i = lane; i < kTileQ * 32; i += 32) {
+    list_d[i] = INFINITY;
+    list_i[i] = 0x7fffffff;
+  }
+  float kth_d = INFINITY;  // lane qq < kTileQ: query qq's current k-th (distance, row)
+  int kth_i = 0x7fffffff;
+  const int nfull = ix.n16 >> 5;
+  const bool half = (ix.n16 & 31) != 0;
+  constexpr int kWarpRows = 8 * kLpR;
+  static_assert(kWarpRows * 32 <= kTileStage, "a stage holds the warp's rows of one block");
+  static_assert(kLpR * kTileQ * 32 <= kTileRing, "the ring holds the parked partials");
+  const int64_t r0 = (int64_t)blockIdx.y * a.chunk_rows, r1 = min(ix.n, r0 + a.chunk_rows);
+  for (int64_t wb = r0 + (int64_t)warp * kWarpRows; wb < r1; wb += (int64_t)kTileWarps * kWarpRows) {
+    // rows past the chunk's end read its last row and are never offered
+    const float* rp[kLpR];
+#pragma unroll
+    for (int r = 0; r < kLpR; ++r) rp[r] = ix.vecs + min(wb + G * kLpR + r, r1 - 1) * ix.pitch;
+    float acc[kLpR][kTileQ];
+#pragma unroll
+    for (int r = 0; r < kLpR; ++r)
+#pragma unroll
+      for (int qq = 0; qq < kTileQ; ++qq) acc[r][qq] = 0.0f;
+    // lane ac copies (and later reads) pieces ac and ac + 4 of its group's rows
+    float* ring = part + (G * kLpR) * 32 + 4 * ac;
+#pragma unroll
+    for (int sb = 0; sb < kTileStages - 1; ++sb) {
+      if (sb < nfull) {
+#pragma unroll
+        for (int r = 0; r < kLpR; ++r) {
+          cp_async16(ring + sb * kTileStage + r * 32, rp[r] + sb * 32 + 4 * ac);
+          cp_async16(ring + sb * kTileStage + r * 32 + 16, rp[r] + sb * 32 + 16 + 4 * ac);
+        }
+      }
+      cp_async_commit();
+    }
+    for (int c = 0; c < nfull; ++c) {
+      const int cb = c + kTileStages - 1;
+      if (cb < nfull) {
+        const int slot = cb % kTileStages;
+#pragma unroll
+        for (int r = 0; r < kLpR; ++r) {
+          cp_async16(ring + slot * kTileStage + r * 32, rp[r] + cb * 32 + 4 * ac);
+          cp_async16(ring + slot * kTileStage + r * 32 + 16, rp[r] + cb * 32 + 16 + 4 * ac);
+        }
+      }
+      cp_async_commit();
+      cp_async_wait_keep<kTileStages - 1>();
+      const float* src = ring + (c % kTileStages) * kTileStage;
+      float4 x0[kLpR], x1[kLpR];
+#pragma unroll
+      for (int r = 0; r < kLpR; ++r) {
+        x0[r] = *reinterpret_cast<const float4*>(src + r * 32);
+        x1[r] = *reinterpret_cast<const float4*>(src + r * 32 + 16);
+      }
+#pragma unroll
+      for (int qq = 0; qq < kTileQ; ++qq) {
+        const float* qb = qs + (size_t)qq * ix.pitch + c * 32 + 4 * ac;
+        const float4 p0 = *reinterpret_cast<const float4*>(qb);
+        const float4 p1 = *reinterpret_cast<const float4*>(qb + 16);
+#pragma unroll
+        for (int r = 0; r < kLpR; ++r) {
+          float t = acc[r][qq];
+          t = lp_term<kL1>(t, p0.x, x0[r].x);
+          t = lp_term<kL1>(t, p1.x, x1[r].x);
+          t = lp_term<kL1>(t, p0.y, x0[r].y);
+          t = lp_term<kL1>(t, p1.y, x1[r].y);
+          t = lp_term<kL1>(t, p0.z, x0[r].z);
+          t = lp_term<kL1>(t, p1.z, x1[r].z);
+          t = lp_term<kL1>(t, p0.w, x0[r].w);
+          acc[r][qq] = lp_term<kL1>(t, p1.w, x1[r].w);
+        }
+      }
+    }
+    cp_async_wait_keep<0>();
+    __syncwarp();  // every lane is done with the ring before the partials are parked over it
+    if (half) {
+      // the 16-element block: pieces of 2 at positions ac (elements ac, ac+8) and ac+4 (ac+4, ac+12)
+#pragma unroll
+      for (int r = 0; r < kLpR; ++r) {
+        const float2 y0 = __ldg(reinterpret_cast<const float2*>(rp[r] + nfull * 32) + ac);
+        const float2 y1 = __ldg(reinterpret_cast<const float2*>(rp[r] + nfull * 32) + ac + 4);
+#pragma unroll
+        for (int qq = 0; qq < kTileQ; ++qq) {
+          const float2 p0 = reinterpret_cast<const float2*>(qs + (size_t)qq * ix.pitch + nfull * 32)[ac];
+          const float2 p1 = reinterpret_cast<const float2*>(qs + (size_t)qq * ix.pitch + nfull * 32)[ac + 4];
+          float t = acc[r][qq];
+          t = lp_term<kL1>(t, p0.x, y0.x);
+          t = lp_term<kL1>(t, p1.x, y1.x);
+          t = lp_term<kL1>(t, p0.y, y0.y);
+          acc[r][qq] = lp_term<kL1>(t, p1.y, y1.y);
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kLpR; ++r)
+#pragma unroll
+      for (int qq = 0; qq < kTileQ; ++qq) part[(r * kTileQ + qq) * 32 + lane] = acc[r][qq];
+    __syncwarp();
+    for (int p = 0; p < kLpR * kTileQ; ++p) {
+      const int r = p / kTileQ, qq = p - r * kTileQ;
+      const int64_t row = wb + G * kLpR + r;
+      const float d = lp_finish4<kL1>(ix, part[p * 32 + lane], ix.vecs + min(row, r1 - 1) * ix.pitch,
+                                      qs + (size_t)qq * ix.pitch);
+      if (qq >= nq_here) continue;
+      const float kd = __shfl_sync(kFull, kth_d, qq);
+      const int ki = __shfl_sync(kFull, kth_i, qq);
+      unsigned m = __ballot_sync(kFull, ac == 0 && row < r1 && scan_better(d, (int)row, kd, ki));
+      if (m) {
+        float bd = list_d[qq * 32 + lane];
+        int bi = list_i[qq * 32 + lane];
+        while (m) {
+          const int src = __ffs(m) - 1;
+          m &= m - 1;
+          scan_offer(bd, bi, a.k, __shfl_sync(kFull, d, src), __shfl_sync(kFull, (int)row, src));
+        }
+        list_d[qq * 32 + lane] = bd;
+        list_i[qq * 32 + lane] = bi;
+        const float nd = __shfl_sync(kFull, bd, a.k - 1);
+        const int ni = __shfl_sync(kFull, bi, a.k - 1);
+        if (lane == qq) {
+          kth_d = nd;
+          kth_i = ni;
+        }
+      }
+    }
+    __syncwarp();  // the next pass overwrites the partials
+  }
+  if (lane < a.k) {
+    const int n_lists = a.n_chunks * kTileWarps;
+    for (int qq = 0; qq < nq_here; ++qq) {
+      const size_t o = ((size_t)(q0 + qq) * n_lists + (size_t)blockIdx.y * kTileWarps + warp) * a.k + lane;
+      a.part_d[o] = list_d[qq * 32 + lane];
+      a.part_id[o] = list_i[qq * 32 + lane];
+    }
+  }
+}
+
 // One warp per query: the best k of its lists, then external ids. The query's lists are one run of
 // n_lists * k entries (a list's unused tail holds the (inf, 0x7fffffff) sentinel); the warp reads
 // 4 x 32 of them at a time, one per lane, and offers only those that beat its current k-th.
@@ -1573,19 +1695,24 @@ __global__ void scan_merge_kernel(const float* __restrict__ part_d, const int32_
 
 }  // namespace
 
-static bool scan_tiled(const DevIndex& ix) {
-  return ix.dist_type == kL2Sqr16Ext || ix.dist_type == kL2SqrExt || ix.dist_type == kNormCosine ||
-         ix.dist_type == kNegDot;
-}
-
-int exact_scan_lists(const DevIndex& ix) { return scan_tiled(ix) ? kTileWarps : 1; }
+int exact_scan_lists(const DevIndex&) { return kTileWarps; }
 
 int exact_scan_knn(const DevIndex& ix, const float* queries, int64_t nq, int k, int kmax, float* part_d,
                    int32_t* part_id, int n_chunks, int32_t* ids, float* dists, int32_t* counts, void* stream) {
   if (nq == 0) return 0;
   if (k < 1 || k > 32) return (int)cudaErrorInvalidValue;
   cudaStream_t st = (cudaStream_t)stream;
-  const int row_bytes = ix.pitch * 4;
+  const int code = ix.dist_type;
+  void (*kern)(ScanArgs) = nullptr;
+  if (code == kL2Sqr16Ext || code == kL2SqrExt) kern = exact_scan_tiled_kernel<true>;
+  else if (code == kNormCosine || code == kNegDot) kern = exact_scan_tiled_kernel<false>;
+  else if (code == kL1) kern = exact_scan_lp_tiled_kernel<true>;
+  else if (code == kLInf) kern = exact_scan_lp_tiled_kernel<false>;
+  else return (int)cudaErrorInvalidValue;
+  const int smem = kTileQ * ix.pitch * 4 + kTileWarps * kTileWarpSmem * 4;
+  if (smem > kMaxDynamicSmem) return (int)cudaErrorInvalidValue;
+  const int rc = allow_max_smem((const void*)kern);
+  if (rc != 0) return rc;
   ScanArgs a;
   a.ix = ix;
   a.queries = queries;
@@ -1595,37 +1722,12 @@ int exact_scan_knn(const DevIndex& ix, const float* queries, int64_t nq, int k, 
   a.chunk_rows = (ix.n + n_chunks - 1) / n_chunks;
   a.part_d = part_d;
   a.part_id = part_id;
-  cudaError_t e;
-  if (scan_tiled(ix)) {
-    a.stage_rows = 0;
-    const int smem = kTileQ * row_bytes + kTileWarps * kTileWarpSmem * 4;
-    if (smem > kMaxDynamicSmem) return (int)cudaErrorInvalidValue;
-    const bool sub = ix.dist_type == kL2Sqr16Ext || ix.dist_type == kL2SqrExt;
-    const void* kern = sub ? (const void*)exact_scan_tiled_kernel<true> : (const void*)exact_scan_tiled_kernel<false>;
-    const int rc = allow_max_smem(kern);
-    if (rc != 0) return rc;
-    const dim3 grid((unsigned)((nq + kTileQ - 1) / kTileQ), (unsigned)n_chunks);
-    if (sub)
-      exact_scan_tiled_kernel<true><<<grid, 32 * kTileWarps, smem, st>>>(a);
-    else
-      exact_scan_tiled_kernel<false><<<grid, 32 * kTileWarps, smem, st>>>(a);
-  } else {
-    // stage at most 32 rows within ~72 KB per block (three blocks per SM even for wide rows:
-    // the loop is latency-bound and needs the warps), at least 4 rows when the rows are wider
-    const int stage_rows =
-        std::max(std::min(32, (72 * 1024 - kScanWarps * row_bytes) / row_bytes) & ~3, 4);
-    if ((stage_rows + kScanWarps) * row_bytes > kMaxDynamicSmem) return (int)cudaErrorInvalidValue;
-    a.stage_rows = stage_rows;
-    const int smem = (stage_rows + kScanWarps) * row_bytes;
-    const int rc = allow_max_smem((const void*)exact_scan_kernel);
-    if (rc != 0) return rc;
-    const dim3 grid((unsigned)((nq + kScanWarps - 1) / kScanWarps), (unsigned)n_chunks);
-    exact_scan_kernel<<<grid, 32 * kScanWarps, smem, st>>>(a);
-  }
-  e = cudaGetLastError();
+  const dim3 grid((unsigned)((nq + kTileQ - 1) / kTileQ), (unsigned)n_chunks);
+  kern<<<grid, 32 * kTileWarps, smem, st>>>(a);
+  const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
-  scan_merge_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(part_d, part_id, nq, n_chunks * exact_scan_lists(ix), k,
-                                                              kmax, ix.ext_id, ids, dists, counts);
+  scan_merge_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(part_d, part_id, nq, n_chunks * kTileWarps, k, kmax,
+                                                              ix.ext_id, ids, dists, counts);
   return (int)cudaGetLastError();
 }
 
