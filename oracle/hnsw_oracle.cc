@@ -30,7 +30,10 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <climits>
 #include <cstring>
+#include <fstream>
+#include <memory>
 #include <queue>
 #include <string>
 #include <thread>
@@ -65,6 +68,8 @@ struct OracleIndex {
   const int32_t* upper(int64_t i, int level) const {
     return links[i].data() + (maxM + 1) * (level - 1);
   }
+  float distance(const float* q, int64_t i) const;
+  int64_t row_bytes() const { return 4LL * dim; }
 };
 
 // ---------------------------------------------------------------- distances
@@ -158,6 +163,48 @@ float dist(int type, const float* q, const float* v, int dim) {
 // (round(v*v) then round(sum + .)), and the scale is the float 1.0f / sqrtf(sum).
 // use_double selects the double-precision sqrt reading, kept only so a test can show that it
 // does not match.
+float OracleIndex::distance(const float* q, int64_t i) const { return dist(dist_type, q, vec(i), dim); }
+
+// ---------------------------------------------------------------- l2sqr_sift (regular index)
+// The objects of space l2sqr_sift: 128 uint8 values and the int sum of their squares
+// (space_l2sqr_sift.cc:137-150); the distance is l2SqrSIFTPrecomp's |a|^2 + |b|^2 - 2 a.b in int
+// (distcomp_l2sqr_sift.cc:40-50; its SSE / AVX forms add the same integers). Every value is at
+// most 128 * 255^2 < 2^24, so the float key the searches carry holds it exactly.
+constexpr int kSiftDim = 128;
+
+struct SiftQuery {
+  const uint8_t* v;
+  int32_t norm;
+};
+
+struct SiftIndex {
+  uint32_t n = 0;
+  int32_t maxlevel = 0;  // the entry point's level: the generic search starts there (hnsw.cc:1183)
+  uint32_t enterpoint = 0;
+  uint64_t M = 0, maxM = 0, maxM0 = 0;
+  std::vector<uint8_t> vecs;  // n x 128
+  std::vector<int32_t> norms, obj_ids;
+  size_t cap0 = 0, capu = 0;
+  std::vector<int32_t> l0s;                 // n x (cap0 + 1): count, then ids
+  std::vector<std::vector<int32_t>> links;  // per node: level x (capu + 1)
+
+  const int32_t* l0(int64_t i) const { return l0s.data() + i * (cap0 + 1); }
+  const int32_t* upper(int64_t i, int level) const { return links[i].data() + (capu + 1) * (level - 1); }
+  float distance(const SiftQuery& q, int64_t i) const {
+    const uint8_t* x = vecs.data() + i * kSiftDim;
+    int32_t dot = 0;
+    for (int e = 0; e < kSiftDim; ++e) dot += int32_t(q.v[e]) * int32_t(x[e]);
+    return (float)(q.norm + norms[i] - 2 * dot);
+  }
+  int64_t row_bytes() const { return kSiftDim + 4; }
+};
+
+int32_t sift_norm(const uint8_t* v) {
+  int32_t s = 0;
+  for (int e = 0; e < kSiftDim; ++e) s += int32_t(v[e]) * int32_t(v[e]);
+  return s;
+}
+
 void normalize(float* v, int dim, int use_double) {
   float sum = 0;
   for (int i = 0; i < dim; ++i) sum = sum + v[i] * v[i];  // -ffp-contract=off: not fused
@@ -285,11 +332,15 @@ struct EvalNode {  // hnsw.h:410-431 — ordered by distance only
 };
 
 // hnsw_distfunc_opt.cc:62-92 / :168-198
-int greedy_descent(const OracleIndex& ix, const float* q, float* curdist_out, Stats& st) {
+// The searches below serve both index kinds: the optimized file (OracleIndex, float rows) and the
+// regular file with l2sqr_sift objects (SiftIndex), whose generic search takes the same steps
+// over node pointers (hnsw.cc:1078-1290 against hnsw_distfunc_opt.cc:48-283).
+template <class Ix, class Q>
+int greedy_descent(const Ix& ix, const Q& q, float* curdist_out, Stats& st) {
   int cur = (int)ix.enterpoint;
-  float curdist = dist(ix.dist_type, q, ix.vec(cur), ix.dim);
+  float curdist = ix.distance(q, cur);
   st.n_dist += 1;
-  st.bytes += 4LL * ix.dim;
+  st.bytes += ix.row_bytes();
   for (int lev = ix.maxlevel; lev > 0; --lev) {
     bool changed = true;
     while (changed) {
@@ -297,11 +348,11 @@ int greedy_descent(const OracleIndex& ix, const float* q, float* curdist_out, St
       const int32_t* data = ix.upper(cur, lev);
       int size = data[0];
       st.n_greedy += 1;
-      st.bytes += 4LL * (1 + size) + 4LL * ix.dim * size;
+      st.bytes += 4LL * (1 + size) + ix.row_bytes() * size;
       st.n_dist += size;
       for (int j = 1; j <= size; ++j) {
         int tnum = data[j];
-        float d = dist(ix.dist_type, q, ix.vec(tnum), ix.dim);
+        float d = ix.distance(q, tnum);
         if (d < curdist) {
           curdist = d;
           cur = tnum;
@@ -314,7 +365,8 @@ int greedy_descent(const OracleIndex& ix, const float* q, float* curdist_out, St
   return cur;
 }
 
-void search_v1merge(const OracleIndex& ix, const float* q, int k, int ef, Visited& vl, Stats& st,
+template <class Ix, class Q>
+void search_v1merge(const Ix& ix, const Q& q, int k, int ef, Visited& vl, Stats& st,
                     std::vector<std::pair<float, int64_t>>& out) {
   vl.reset();
   float curdist;
@@ -339,9 +391,9 @@ void search_v1merge(const OracleIndex& ix, const float* q, int k, int ef, Visite
       int tnum = data[j];
       if (vl.mass[tnum] != vl.cur) {
         vl.mass[tnum] = vl.cur;
-        float d = dist(ix.dist_type, q, ix.vec(tnum), ix.dim);
+        float d = ix.distance(q, tnum);
         st.n_dist += 1;
-        st.bytes += 4LL * ix.dim;
+        st.bytes += ix.row_bytes();
         if (d < topKey || arr.num < (size_t)ef) {
           buff[qty].key = d;
           buff[qty].used = false;
@@ -374,7 +426,8 @@ void search_v1merge(const OracleIndex& ix, const float* q, int k, int ef, Visite
   std::reverse(out.begin(), out.end());
 }
 
-void search_old(const OracleIndex& ix, const float* q, int k, int ef, Visited& vl, Stats& st,
+template <class Ix, class Q>
+void search_old(const Ix& ix, const Q& q, int k, int ef, Visited& vl, Stats& st,
                 std::vector<std::pair<float, int64_t>>& out) {
   vl.reset();
   float curdist;
@@ -399,9 +452,9 @@ void search_old(const OracleIndex& ix, const float* q, int k, int ef, Visited& v
       int tnum = data[j];
       if (vl.mass[tnum] != vl.cur) {
         vl.mass[tnum] = vl.cur;
-        float d = dist(ix.dist_type, q, ix.vec(tnum), ix.dim);
+        float d = ix.distance(q, tnum);
         st.n_dist += 1;
-        st.bytes += 4LL * ix.dim;
+        st.bytes += ix.row_bytes();
         if (closest.top().distance > d || closest.size() < (size_t)ef) {
           cand.push({-d, tnum});
           rq.offer(d, tnum);
@@ -543,6 +596,157 @@ int oracle_search(void* h, const float* queries, int64_t nq, int dim, int k, con
         stats[qi * 4 + 1] = st.n_expand;
         stats[qi * 4 + 2] = st.n_greedy;
         stats[qi * 4 + 3] = st.bytes;
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthreads; ++t) th.emplace_back(worker);
+  for (auto& t : th) t.join();
+  return 0;
+}
+
+// Reads an l2sqr_sift index: the regular graph file written by SaveRegularIndexBin
+// (hnsw.cc:810-842: u32 0 | u32 N | i32 maxlevel | u32 entry | u64 M | u64 maxM | u64 maxM0, then per
+// node u32 level and, for each level 0..level, u32 count and the neighbour ids) and the objects
+// file written by saveIndex(..., save_data=True) (python_bindings/nmslib.cc:115-125, space.cc:90-104:
+// u64 count, then per object u64 length and the object: i32 id | i32 label | u64 datalength |
+// 128 uint8 | i32 norm). Returns null with the reason in oracle_last_error().
+void* oracle_sift_load(const char* graph_path, const char* data_path) {
+  auto ix = std::make_unique<SiftIndex>();
+  std::ifstream dat(data_path, std::ios::binary);
+  if (!dat) {
+    g_err = std::string("cannot open ") + data_path;
+    return nullptr;
+  }
+  uint64_t qty = 0;
+  dat.read(reinterpret_cast<char*>(&qty), 8);
+  ix->vecs.resize(qty * kSiftDim);
+  ix->norms.resize(qty);
+  ix->obj_ids.resize(qty);
+  for (uint64_t i = 0; i < qty; ++i) {
+    uint64_t len = 0, dlen = 0;
+    int32_t id = 0, label = 0;
+    dat.read(reinterpret_cast<char*>(&len), 8);
+    dat.read(reinterpret_cast<char*>(&id), 4);
+    dat.read(reinterpret_cast<char*>(&label), 4);
+    dat.read(reinterpret_cast<char*>(&dlen), 8);
+    if (!dat || dlen != kSiftDim + 4 || len != 16 + dlen) {
+      g_err = "objects file: not a 128-byte l2sqr_sift object at position " + std::to_string(i);
+      return nullptr;
+    }
+    dat.read(reinterpret_cast<char*>(ix->vecs.data() + i * kSiftDim), kSiftDim);
+    dat.read(reinterpret_cast<char*>(&ix->norms[i]), 4);
+    ix->obj_ids[i] = id;
+  }
+  if (!dat) {
+    g_err = "objects file is truncated";
+    return nullptr;
+  }
+  std::ifstream g(graph_path, std::ios::binary);
+  uint32_t flag = 1, n = 0;
+  g.read(reinterpret_cast<char*>(&flag), 4);
+  g.read(reinterpret_cast<char*>(&n), 4);
+  g.read(reinterpret_cast<char*>(&ix->maxlevel), 4);
+  g.read(reinterpret_cast<char*>(&ix->enterpoint), 4);
+  g.read(reinterpret_cast<char*>(&ix->M), 8);
+  g.read(reinterpret_cast<char*>(&ix->maxM), 8);
+  g.read(reinterpret_cast<char*>(&ix->maxM0), 8);
+  if (!g || flag != 0 || n != qty || (n && ix->enterpoint >= n)) {
+    g_err = "graph file: not a regular index over these objects";
+    return nullptr;
+  }
+  ix->n = n;
+  std::vector<std::vector<std::vector<int32_t>>> lists(n);
+  size_t cap0 = ix->maxM0, capu = ix->maxM;
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t level = 0;
+    g.read(reinterpret_cast<char*>(&level), 4);
+    if (!g || level > 64) {
+      g_err = "graph file: bad level at node " + std::to_string(i);
+      return nullptr;
+    }
+    lists[i].resize(level + 1);
+    for (uint32_t lev = 0; lev <= level; ++lev) {
+      uint32_t cnt = 0;
+      g.read(reinterpret_cast<char*>(&cnt), 4);
+      if (!g || cnt > n) {
+        g_err = "graph file: bad list at node " + std::to_string(i);
+        return nullptr;
+      }
+      lists[i][lev].resize(cnt);
+      g.read(reinterpret_cast<char*>(lists[i][lev].data()), 4LL * cnt);
+      for (int32_t f : lists[i][lev])
+        if (f < 0 || (uint32_t)f >= n) {
+          g_err = "graph file: neighbour id out of range at node " + std::to_string(i);
+          return nullptr;
+        }
+      (lev ? capu : cap0) = std::max<size_t>(lev ? capu : cap0, cnt);
+    }
+  }
+  if (!g) {
+    g_err = "graph file is truncated";
+    return nullptr;
+  }
+  ix->cap0 = cap0;
+  ix->capu = capu;
+  ix->l0s.assign((size_t)n * (cap0 + 1), 0);
+  ix->links.resize(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    int32_t* d = ix->l0s.data() + (size_t)i * (cap0 + 1);
+    d[0] = (int32_t)lists[i][0].size();
+    std::copy(lists[i][0].begin(), lists[i][0].end(), d + 1);
+    const size_t levels = lists[i].size() - 1;
+    ix->links[i].assign(levels * (capu + 1), 0);
+    for (size_t lev = 1; lev <= levels; ++lev) {
+      int32_t* u = ix->links[i].data() + (lev - 1) * (capu + 1);
+      u[0] = (int32_t)lists[i][lev].size();
+      std::copy(lists[i][lev].begin(), lists[i][lev].end(), u + 1);
+    }
+  }
+  if (n) ix->maxlevel = (int32_t)lists[ix->enterpoint].size() - 1;
+  return ix.release();
+}
+
+void oracle_sift_free(void* h) { delete static_cast<SiftIndex*>(h); }
+
+// info: n, maxlevel (the entry point's), entry point, M, maxM, maxM0
+void oracle_sift_info(void* h, int64_t* info) {
+  auto* ix = static_cast<SiftIndex*>(h);
+  info[0] = ix->n;
+  info[1] = ix->maxlevel;
+  info[2] = ix->enterpoint;
+  info[3] = (int64_t)ix->M;
+  info[4] = (int64_t)ix->maxM;
+  info[5] = (int64_t)ix->maxM0;
+}
+
+// Batch search over nq x 128 uint8 queries; algo as oracle_search. Outputs nq x kmax object ids
+// and int distances, -1 / INT32_MAX padding.
+int oracle_sift_search(void* h, const uint8_t* queries, int64_t nq, int k, int ef, int algo, int kmax, int32_t* ids,
+                       int32_t* dists, int32_t* counts, int nthreads) {
+  auto* ix = static_cast<SiftIndex*>(h);
+  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  std::atomic<int64_t> next(0);
+  auto worker = [&]() {
+    Visited vl(ix->n);
+    std::vector<std::pair<float, int64_t>> res;
+    for (;;) {
+      const int64_t qi = next.fetch_add(1);
+      if (qi >= nq) break;
+      Stats st;
+      res.clear();
+      if (ix->n) {
+        const SiftQuery q{queries + qi * kSiftDim, sift_norm(queries + qi * kSiftDim)};
+        if (algo == 1 || (algo == 0 && ef >= 1000))
+          search_old(*ix, q, k, ef, vl, st, res);
+        else
+          search_v1merge(*ix, q, k, ef, vl, st, res);
+      }
+      const int cnt = (int)std::min<size_t>(res.size(), (size_t)kmax);
+      counts[qi] = cnt;
+      for (int j = 0; j < kmax; ++j) {
+        ids[qi * kmax + j] = j < cnt ? ix->obj_ids[res[j].second] : -1;
+        dists[qi * kmax + j] = j < cnt ? (int32_t)res[j].first : INT32_MAX;
       }
     }
   };

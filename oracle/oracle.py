@@ -8,6 +8,10 @@ ground truth. Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline 
   hnsw.cc:1025-1074) and searches it with the reference's SearchV1Merge / SearchOld semantics
   (src/method/hnsw_distfunc_opt.cc:46-283), FMA lane order of
   include/method/hnsw_distfunc_opt_impl_inline.h:42-173.
+* ``OracleSiftIndex`` — loads an ``l2sqr_sift`` index (the regular graph file of
+  hnsw.cc:810-842 and the ``<file>.dat`` objects of python_bindings/nmslib.cc:115-125) and
+  searches it with the same steps (the generic search of hnsw.cc:1078-1290) and the reference's
+  int distance (distcomp_l2sqr_sift.cc:40-50).
 * ``bruteforce_fp64`` — exact kNN in float64 with ties broken by id; the recall ground truth.
 * ``reference_module`` — the reference's own pybind module built by ``make -C oracle ref``
   into ``oracle/_ref`` (present only where the reference sources were available to build it).
@@ -55,6 +59,12 @@ def _load():
         lib.oracle_search.restype = I32
         lib.oracle_search.argtypes = [P, P, I64, I32, I32, P, I32, P, I32, I32, P, P, P, P, I32]
         lib.oracle_std_sort_items.argtypes = [P, P, I32]
+        lib.oracle_sift_load.restype = P
+        lib.oracle_sift_load.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        lib.oracle_sift_free.argtypes = [P]
+        lib.oracle_sift_info.argtypes = [P, P]
+        lib.oracle_sift_search.restype = I32
+        lib.oracle_sift_search.argtypes = [P, P, I64, I32, I32, I32, I32, P, P, P, I32]
         lib.oracle_last_error.restype = ctypes.c_char_p
         _lib = lib
     return _lib
@@ -137,6 +147,42 @@ def std_sort_items(keys, payload):
     p = np.array(payload, np.int32, copy=True)
     _load().oracle_std_sort_items(_ptr(k), _ptr(p), k.shape[0])
     return k, p
+
+
+class OracleSiftIndex:
+    """CPU restatement of the reference's generic HNSW search over an ``l2sqr_sift`` index: 128
+    uint8 values per object, int distances."""
+
+    INFO_KEYS = ("n", "maxlevel", "enterpoint", "M", "maxM", "maxM0")
+
+    def __init__(self, path: str, data_path: str | None = None):
+        lib = _load()
+        self._h = lib.oracle_sift_load(path.encode(), (data_path or path + ".dat").encode())
+        if not self._h:
+            raise ValueError(lib.oracle_last_error().decode())
+        info = np.zeros(len(self.INFO_KEYS), np.int64)
+        lib.oracle_sift_info(self._h, _ptr(info))
+        self.info = dict(zip(self.INFO_KEYS, (int(v) for v in info)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _load().oracle_sift_free(self._h)
+            self._h = None
+
+    def search(self, queries, k, ef, algo=0, nthreads=0):
+        """(ids [nq,k], int32 dists [nq,k], counts [nq]); algo 0 hybrid, 1 old, 2 v1merge."""
+        q = np.ascontiguousarray(queries, np.uint8)
+        if q.ndim != 2 or q.shape[1] != 128:
+            raise ValueError("l2sqr_sift queries are [nq, 128] uint8")
+        nq = q.shape[0]
+        ids = np.empty((nq, k), np.int32)
+        dists = np.empty((nq, k), np.int32)
+        counts = np.empty(nq, np.int32)
+        rc = _load().oracle_sift_search(self._h, _ptr(q), nq, int(k), int(ef), int(algo), int(k), _ptr(ids),
+                                        _ptr(dists), _ptr(counts), int(nthreads))
+        if rc != 0:
+            raise ValueError(_load().oracle_last_error().decode())
+        return ids, dists, counts
 
 
 def bruteforce_fp64(base, queries, k, space, ids=None, chunk=256):
