@@ -4,19 +4,24 @@ Workload (default): 1M x 128 SIFT-like float32 base (seeded synthetic stand-in f
 10K queries, space l2, M=16, efConstruction=200, k=10, efSearch swept over
 {16, 32, 64, 128, 256, 512}; the headline efSearch is the smallest one whose recall@10 reaches
 0.95 against exact float64 neighbours. One step = one batch of 10K queries through the engine.
+The index is built by the reference's own createIndex and written by its saveIndex (cached per
+machine); both arms load that same file.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line (rank 0). ``value`` is device-timed throughput with queries resident in HBM;
 ``e2e`` is the same metric through the public Python API with host arrays (H2D of the queries and
-D2H of ids/distances/counts inside the timed region). ``--impl reference`` times the reference's
-own CPU knnQueryBatch (built from its sources into oracle/_ref) on the same index and queries.
-Multi-GPU runs are replicas (the query path has no exchange step): each rank searches its own
-batch against its own copy of the index and ``value`` sums the queries of all ranks.
+D2H of ids/distances/counts inside the timed region). ``parity`` compares the engine's lists with
+the reference's knnQueryBatch on the same file at full size. ``--impl reference`` times the
+reference's own CPU knnQueryBatch (built from its sources into oracle/_ref) on the same index and
+queries, and loads nothing of the engine. Multi-GPU runs are replicas (the query path has no
+exchange step): each rank searches its own batch against its own copy of the index and ``value``
+sums the queries of all ranks.
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import re
@@ -89,52 +94,95 @@ def replica_throughput(nq_per_rank, ms_per_rank, world):
 
 
 # ------------------------------------------------------------------ data and index
-def workload_data():
-    from nmslib_b200.datasets import workload
-    base, queries, space, m = workload(WORKLOAD)
-    return base, queries, space, m
+def _datasets():
+    """nmslib_b200/datasets.py loaded by file path, so the reference arm imports nothing of the
+    engine's package."""
+    spec = importlib.util.spec_from_file_location("_bench_datasets", os.path.join(ROOT, "nmslib_b200", "datasets.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
-def index_path(m):
-    return os.path.join(CACHE_DIR, f"{WORKLOAD}_M{m}_efc{EFC}_seed0.hnsw")
+def workload_data(name=WORKLOAD):
+    return _datasets().workload(name)
 
 
-HOST_BUILD_SECONDS = None
+def index_path(name, m):
+    return os.path.join(CACHE_DIR, f"{name}_M{m}_efc{EFC}_reference_build.hnsw")
 
 
-def ensure_index(base, space, m, rank, world):
-    """Rank 0 builds the index with the engine's host builder (all host cores) unless a copy is
-    cached on this machine; the other ranks wait and load the same file."""
-    global HOST_BUILD_SECONDS
-    from nmslib_b200 import SPACES, _capi
-    path = index_path(m)
+BUILD_INFO = {}
+
+
+def reference_module_or_none():
+    from oracle.oracle import reference_module
+    return reference_module()
+
+
+def ensure_index(name, base, space, m, rank, world):
+    """Rank 0 builds the index with the reference's own createIndex (all host cores) and writes it
+    with its saveIndex, unless a copy is cached on this machine; the other ranks wait and load the
+    same file. Returns the path, or None when the reference module is not available."""
+    path = index_path(name, m)
     if rank == 0 and not os.path.exists(path):
+        ref = reference_module_or_none()
+        if ref is not None:
+            os.makedirs(CACHE_DIR, exist_ok=True)
+            threads = os.cpu_count() or 1
+            t0 = time.time()
+            idx = ref.init(method="hnsw", space=space)
+            idx.addDataPointBatch(base)
+            idx.createIndex({"M": m, "efConstruction": EFC, "indexThreadQty": threads}, print_progress=False)
+            idx.saveIndex(path + ".tmp", save_data=False)
+            del idx
+            os.replace(path + ".tmp", path)
+            BUILD_INFO[name] = {"seconds": round(time.time() - t0, 1), "threads": threads}
+            log(f"[bench] reference createIndex {name}: {BUILD_INFO[name]}")
+    barrier(world)
+    return path if os.path.exists(path) else None
+
+
+def engine_built_index(name, base, space, m):
+    """Fallback when the reference module is missing: the engine's host builder (labelled so)."""
+    from nmslib_b200 import SPACES, _capi
+    path = os.path.join(CACHE_DIR, f"{name}_M{m}_efc{EFC}_engine_build.hnsw")
+    if not os.path.exists(path):
         os.makedirs(CACHE_DIR, exist_ok=True)
-        t0 = time.time()
         _capi.build_index(base, SPACES[space], m, EFC, nthreads=0, seed=0, out_path=path + ".tmp")
         os.replace(path + ".tmp", path)
-        HOST_BUILD_SECONDS = time.time() - t0
-        log(f"[bench] built {path} in {HOST_BUILD_SECONDS:.1f}s")
-    barrier(world)
     return path
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def ground_truth(base, queries, k):
-    """Exact float64 neighbours on the GPU (measurement only): ids [nq, k] and the k-th distance."""
+    """Exact float64 neighbours on the GPU (measurement only): ids [nq, k], the k-th distance and
+    the k smallest squared distances [nq, k] (ascending)."""
     import torch
     b = torch.from_numpy(base).cuda().double()
     bsq = (b * b).sum(1)
     kth = np.empty(len(queries))
     ids = np.empty((len(queries), k), np.int64)
+    dk = np.empty((len(queries), k))
     for s in range(0, len(queries), 512):
         q = torch.from_numpy(queries[s:s + 512]).cuda().double()
         d = (q * q).sum(1, keepdim=True) - 2 * q @ b.T + bsq[None, :]
         v, i = torch.topk(d, k, dim=1, largest=False)
         ids[s:s + 512] = i.cpu().numpy()
         kth[s:s + 512] = v[:, -1].cpu().numpy()
+        dk[s:s + 512] = v.cpu().numpy()
     del b
     torch.cuda.empty_cache()
-    return ids, kth
+    return ids, kth, dk
 
 
 def recall_at_k(found_d, counts, kth, k):
@@ -143,6 +191,56 @@ def recall_at_k(found_d, counts, kth, k):
     valid = np.arange(found_d.shape[1])[None, :k] < np.minimum(counts, k)[:, None]
     ok = found_d[:, :k] <= (kth * (1 + 1e-6) + 1e-6)[:, None]
     return float(np.sum(valid & ok)) / (k * len(kth))
+
+
+def list_parity(ids_a, d_a, cnt_a, ids_b, d_b, cnt_b):
+    """Result lists a (the engine) against b (the reference), both ascending by distance:
+    identical lists; lists whose ids differ only inside runs of equal distance (including the run
+    cut by k, where either side may keep any of the tied items); and the largest relative distance
+    difference position by position."""
+    n = len(cnt_a)
+    identical = tie_only = other = 0
+    max_rel = 0.0
+    for r in range(n):
+        ca, cb = int(cnt_a[r]), int(cnt_b[r])
+        if ca != cb:
+            other += 1
+            continue
+        da, db = d_a[r, :ca].astype(np.float64), d_b[r, :cb].astype(np.float64)
+        if ca:
+            max_rel = max(max_rel, float((np.abs(da - db) / np.maximum(np.abs(db), 1e-30)).max()))
+        ia, ib = ids_a[r, :ca], ids_b[r, :cb]
+        if (ia == ib).all():
+            identical += 1
+            continue
+        ok = bool((da == db).all())
+        s0 = 0
+        while ok and s0 < ca:
+            e = s0
+            while e < ca and db[e] == db[s0]:
+                e += 1
+            if e < ca and sorted(ia[s0:e].tolist()) != sorted(ib[s0:e].tolist()):
+                ok = False
+            s0 = e
+        if ok:
+            tie_only += 1
+        else:
+            other += 1
+    return {"queries": n, "identical_lists_frac": identical / max(1, n), "tie_only_frac": tie_only / max(1, n),
+            "other_frac": other / max(1, n), "max_rel_dist": max_rel}
+
+
+def reference_arrays(ref_index, queries, k, threads):
+    """The reference's knnQueryBatch as dense arrays (ids, dists, counts), ascending."""
+    res = ref_index.knnQueryBatch(queries, k=k, num_threads=threads)
+    ids = np.full((len(res), k), -1, np.int32)
+    dd = np.full((len(res), k), np.inf, np.float32)
+    cnt = np.zeros(len(res), np.int32)
+    for r, (i, d) in enumerate(res):
+        ids[r, :len(i)] = i
+        dd[r, :len(d)] = d
+        cnt[r] = len(i)
+    return ids, dd, cnt
 
 
 # ------------------------------------------------------------------ clocks
@@ -214,10 +312,10 @@ def peaks():
 
 
 # ------------------------------------------------------------------ reference (CPU) arm
-def cpu_reference_qps(path, queries, ef, k, target_seconds=3.0, space="l2"):
-    """The reference's own knnQueryBatch on all host cores over a bounded sample of the batch
-    (sized to about `target_seconds` per run, best of 3 runs as benchmark/eval.py:489-508 does).
-    Returns (qps, sample_size, kind, cores)."""
+def cpu_reference_qps(path, queries, ef, k, target_seconds=3.0, space="l2", one_thread=True):
+    """The reference's own knnQueryBatch on the host cores over a bounded sample of the batch
+    (sized to about `target_seconds` per run, best of 3 runs as benchmark/eval.py:489-508 does),
+    with every core and, when `one_thread`, with one thread. Returns a dict."""
     from oracle.oracle import OracleIndex, reference_module
     cores = os.cpu_count() or 1
     ref = reference_module()
@@ -225,24 +323,35 @@ def cpu_reference_qps(path, queries, ef, k, target_seconds=3.0, space="l2"):
         idx = ref.init(method="hnsw", space=space)
         idx.loadIndex(path)
         idx.setQueryTimeParams({"efSearch": ef})
-        run = lambda q: idx.knnQueryBatch(q, k=k, num_threads=cores)  # noqa: E731
+        run = lambda q, t: idx.knnQueryBatch(q, k=k, num_threads=t)  # noqa: E731
         kind = "reference"
     else:
         oix = OracleIndex(path)
-        run = lambda q: oix.search(q, k=k, ef=ef, nthreads=cores)  # noqa: E731
+        run = lambda q, t: oix.search(q, k=k, ef=ef, nthreads=t)  # noqa: E731
         kind = "port"
-    n = min(len(queries), 1000)
-    t0 = time.perf_counter()
-    run(queries[:n])  # warm-up and sizing
-    dt = time.perf_counter() - t0
-    n = int(min(len(queries), max(n, n * target_seconds / max(dt, 1e-6))))
-    best = None
-    for _ in range(3):
+
+    def best_qps(threads, seconds):
+        n = min(len(queries), 1000 if threads > 1 else 200)
         t0 = time.perf_counter()
-        run(queries[:n])
+        run(queries[:n], threads)  # warm-up and sizing
         dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
-    return n / best, n, kind, cores
+        n = int(min(len(queries), max(n, n * seconds / max(dt, 1e-6))))
+        best = None
+        for _ in range(3):
+            t0 = time.perf_counter()
+            run(queries[:n], threads)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        return n / best, n
+
+    qps, n = best_qps(cores, target_seconds)
+    out = {"value": qps, "unit": "queries/s", "cores": cores, "kind": kind, "cpu_model": cpu_model(),
+           "sample": f"best of 3 knnQueryBatch(num_threads={cores}) over {n} of the {len(queries)} queries, "
+                     f"efSearch={ef}"}
+    if one_thread:
+        q1, n1 = best_qps(1, 1.0)
+        out["one_thread"] = {"value": q1, "sample": f"best of 3 knnQueryBatch(num_threads=1) over {n1} queries"}
+    return out
 
 
 # ------------------------------------------------------------------ serving and brute force
@@ -277,10 +386,13 @@ def serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6), seconds=1.0, seed
             "memory_budget_bytes": budget}
 
 
-def brute_force_measure(index, queries, k=10, reps=3):
+def brute_force_measure(index, queries, k=10, reps=3, base=None, true_d=None, space="l2"):
     """Exact k-NN of the whole batch over every stored vector: time and throughput. The tensor-core
     path (l2 / cosine / negdot, dim <= 256) reports 2 * nq * n * padded dim BF16 FLOP per batch; the
-    exact CUDA-core scan (L1, LInf, wider rows) 2 * nq * n * dim FP32 FLOP."""
+    exact CUDA-core scan (L1, LInf, wider rows) 2 * nq * n * dim FP32 FLOP. With `base` and the
+    float64 top-k distances `true_d` [nq, k] (l2), every query's returned set is checked: the
+    float64 distances of the returned ids must be the float64 top-k distances (exact top-k up to
+    the choice among equal distances)."""
     import torch
     ids, d, c, st = index.bruteForceBatchArrays(queries, k, stats=True)  # builds the BF16 copy
     t = []
@@ -302,8 +414,64 @@ def brute_force_measure(index, queries, k=10, reps=3):
                "ms_end_to_end": round(best * 1e3, 3), "qps": round(len(queries) / best),
                "tensor_tflops": round(flops / best / 1e12, 1), "sample_rows": int(st[0]),
                "max_rows_reranked": int(st[1]), "rescanned": int(st[2])}
+    if base is not None and true_d is not None and space == "l2":
+        res["verify_fp64"] = bf_verify_l2(base, queries, ids, c, true_d)
+        res["bf16_key_error"] = bf16_key_error_l2(base, queries[:256])
     log(f"[bench] brute force: {res}")
     return res
+
+
+def bf_verify_l2(base, queries, ids, counts, true_d):
+    """Float64 squared distances of the returned ids against the float64 top-k: the fraction of
+    queries whose returned distances equal the true k smallest, position by position."""
+    import torch
+    b = torch.from_numpy(base).cuda()
+    exact = 0
+    worst = 0.0
+    k = true_d.shape[1]
+    for s0 in range(0, len(queries), 1024):
+        q = torch.from_numpy(queries[s0:s0 + 1024]).cuda().double()
+        i = torch.from_numpy(ids[s0:s0 + 1024, :k].astype(np.int64)).cuda()
+        x = b[i.clamp_min(0)].double()
+        d = ((x - q[:, None, :]) ** 2).sum(-1)
+        d = torch.where(i >= 0, d, torch.full_like(d, float("inf")))
+        d, _ = torch.sort(d, dim=1)
+        t = torch.from_numpy(true_d[s0:s0 + 1024]).cuda()
+        ok = (d == t).all(dim=1) & torch.from_numpy(counts[s0:s0 + 1024] == k).cuda()
+        exact += int(ok.sum().item())
+        worst = max(worst, float(((d - t).abs() / t.abs().clamp_min(1e-30)).max().item()))
+    del b
+    torch.cuda.empty_cache()
+    return {"queries": len(queries), "exact_topk_frac": exact / max(1, len(queries)), "max_rel_dist_err": worst}
+
+
+def bf16_key_error_l2(base, queries):
+    """Largest |BF16 key - float64 key| of the tensor-core pass over every base row for a sample of
+    queries: key = 2 q.x - |x|^2 with q and x rounded to BF16 and the product summed in FP32 (the
+    GEMM's inputs and accumulator type), against the same key in float64. The rerank removes this
+    error; the bound the kernel uses to pick candidates covers it."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        b32 = torch.from_numpy(base).cuda()
+        bb = b32.bfloat16().float()
+        xn = (b32 * b32).sum(1)
+        b64 = b32.double()
+        xn64 = (b64 * b64).sum(1)
+        worst = 0.0
+        scale = 0.0
+        for s0 in range(0, len(queries), 64):
+            q = torch.from_numpy(queries[s0:s0 + 64]).cuda()
+            kb = 2.0 * (q.bfloat16().float() @ bb.T) - xn[None, :]
+            k64 = 2.0 * (q.double() @ b64.T) - xn64[None, :]
+            worst = max(worst, float((kb.double() - k64).abs().max().item()))
+            scale = max(scale, float(k64.abs().max().item()))
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    torch.cuda.empty_cache()
+    return {"queries": len(queries), "max_abs_key_err": worst, "max_abs_key": scale,
+            "key": "2 q.x - |x|^2, BF16 inputs, FP32 accumulation"}
 
 
 def profile_scan(n, calls, dim=960, nq=200):
@@ -334,9 +502,9 @@ def profile_scan(n, calls, dim=960, nq=200):
         f"({2.0 * nq * n * dim / best / 1e12:.1f} TFLOP/s end to end)")
 
 
-def build_compare(base, space, m, queries, kth, host_recall, device):
-    """The same index built with the level-0 construction searches on the GPU: wall time and
-    recall@10 at the headline efSearch, beside the host build's."""
+def build_compare(base, space, m, queries, kth, ref_recall, device):
+    """The same index built by the engine with the level-0 construction searches on the GPU: wall
+    time and recall@10 at the headline efSearch, beside the reference build's."""
     import nmslib_b200 as nmslib
     from nmslib_b200 import SPACES, _capi
     path = os.path.join(CACHE_DIR, f"{WORKLOAD}_M{m}_efc{EFC}_device_build.hnsw")
@@ -350,9 +518,10 @@ def build_compare(base, space, m, queries, kth, host_recall, device):
     rec = recall_at_k(dd, cnt, kth, K)
     del idx
     os.remove(path)
-    res = {"host_build_s": None if HOST_BUILD_SECONDS is None else round(HOST_BUILD_SECONDS, 2),
+    ref_build = BUILD_INFO.get(WORKLOAD)
+    res = {"reference_build_s": ref_build["seconds"] if ref_build else None,
            "device_build_s": round(dt, 2), "host_threads": os.cpu_count(),
-           f"recall@10_ef{HEADLINE_EF}": {"host_build": round(host_recall, 4), "device_build": round(rec, 4)}}
+           f"recall@10_ef{HEADLINE_EF}": {"reference_build": round(ref_recall, 4), "device_build": round(rec, 4)}}
     log(f"[bench] index build: {res}")
     return res
 
@@ -430,8 +599,10 @@ def run_aux(args):
             log(f"[bench] {name} ef={ef}: {rows[-1]}")
         out["hnsw"] = rows
         ef_ref = 200 if args.workload == "c3" else 100
-        qps, n, kind, cores = cpu_reference_qps(path, qs, ef_ref, 10, space=space)
-        out["cpu_reference"] = {"efSearch": ef_ref, "qps": round(qps), "cores": cores, "kind": kind, "sample": n}
+        cpu = cpu_reference_qps(path, qs, ef_ref, 10, space=space)
+        out["cpu_reference"] = {"efSearch": ef_ref, "qps": round(cpu["value"]), "cores": cpu["cores"],
+                                "kind": cpu["kind"], "sample": cpu["sample"],
+                                "one_thread_qps": round(cpu["one_thread"]["value"])}
     if args.workload == "c3":
         out["bruteforce"] = brute_force_measure(index, queries[:10_000])
     if args.workload == "c5":
@@ -472,11 +643,6 @@ def run_aux(args):
     print(json.dumps(out))
 
 
-def reference_module_or_none():
-    from oracle.oracle import reference_module
-    return reference_module()
-
-
 # ------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -508,19 +674,25 @@ def main():
     base, queries, space, m = workload_data()
 
     if args.impl == "reference":
+        # the reference alone: its createIndex builds the file (or a cached copy is read), its
+        # knnQueryBatch is timed; nothing of the engine is imported or loaded
         if rank != 0:
             return
-        path = ensure_index(base, space, m, 0, 1)
+        if reference_module_or_none() is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference module not built (oracle/_ref)"}))
+            return
+        path = ensure_index(WORKLOAD, base, space, m, 0, 1)
         ef = HEADLINE_EF
-        qps, n, kind, cores = cpu_reference_qps(path, queries, ef, K, space=space)
+        cpu = cpu_reference_qps(path, queries, ef, K, space=space)
+        qps = cpu["value"]
         ms = 1e3 * len(queries) / qps
         line = {"metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
                 "config": {"workload": WORKLOAD, "n_base": len(base), "nq": len(queries), "dim": base.shape[1],
-                           "M": m, "efConstruction": EFC, "efSearch": ef, "k": K},
-                "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "kind": kind,
-                                 "sample": f"best of repeated knnQueryBatch over {n} of the {len(queries)} queries"},
+                           "M": m, "efConstruction": EFC, "efSearch": ef, "k": K,
+                           "index_builder": "reference createIndex", "index_build": BUILD_INFO.get(WORKLOAD)},
+                "cpu_baseline": cpu,
                 "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -532,7 +704,14 @@ def main():
     from nmslib_b200.build import build
     build()
     torch.cuda.set_device(local)
-    path = ensure_index(base, space, m, rank, world)
+    path = ensure_index(WORKLOAD, base, space, m, rank, world)
+    index_builder = "reference createIndex"
+    if path is None:  # no reference module on this machine: the engine's own builder, labelled so
+        index_builder = "nmslib_b200 host builder (reference module unavailable)"
+        if rank == 0:
+            engine_built_index(WORKLOAD, base, space, m)
+        barrier(world)
+        path = engine_built_index(WORKLOAD, base, space, m)
     index = nmslib.init(method="hnsw", space=space, device=local)
     index.loadIndex(path)
     lib = _capi.load()
@@ -580,7 +759,7 @@ def main():
         return
 
     # ---- untimed: recall / throughput sweep, headline ef
-    gt_ids, kth = ground_truth(base, queries, K)
+    gt_ids, kth, true_d = ground_truth(base, queries, K)
     sweep = []
     for ef in EF_SWEEP:
         index.setQueryTimeParams({"efSearch": ef})
@@ -638,12 +817,18 @@ def main():
     e2e_ms = max_over_ranks(e2e_ms, world)
     e2e = world * nq / (e2e_ms * 1e-3)
 
+    # ---- full-size parity against the reference's knnQueryBatch on the same file (checker)
+    parity = None
+    if rank == 0 and world == 1:
+        parity = full_size_parity(index, path, queries, space, (HEADLINE_EF, 256))
+        parity["c1_gauss10k_d128_l2"] = c1_parity(local)
+
     # ---- serving: open-loop Poisson arrivals of the serving mix (batch 1..256 log-uniform,
     # k in {10, 100}, efSearch in {100, 400}) against the same resident index
     serving = serve_sweep(index, queries) if world == 1 else None
 
-    # ---- exact brute force on the tensor cores (same queries and vectors)
-    brute = brute_force_measure(index, queries) if world == 1 else None
+    # ---- exact brute force on the tensor cores (same queries and vectors), checked against float64
+    brute = brute_force_measure(index, queries, base=base, true_d=true_d, space=space) if world == 1 else None
 
     # ---- the index built again with the construction searches on the GPU
     build_info = build_compare(base, space, m, queries, kth, head["recall@10"], local) if world == 1 else None
@@ -653,10 +838,7 @@ def main():
     traffic = recorded_traffic()
     cpu = None
     if rank == 0 and world == 1:
-        qps, n, kind, cores = cpu_reference_qps(path, queries, ef, K, space=space)
-        cpu = {"value": qps, "unit": "queries/s", "cores": cores, "kind": kind,
-               "sample": f"best of repeated knnQueryBatch(num_threads={cores}) over {n} of the {nq} queries, "
-                         f"efSearch={ef}"}
+        cpu = cpu_reference_qps(path, queries, ef, K, space=space)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
@@ -664,7 +846,7 @@ def main():
                 "config": {"workload": WORKLOAD, "n_base": len(base), "nq_per_gpu": nq, "dim": dim, "M": m,
                            "efConstruction": EFC, "efSearch": ef, "k": K, "recall@10": head["recall@10"],
                            "parallelism": f"replicas x{world}", "l2_flush": "no: index (512 MB) > L2 (126 MB)",
-                           "index_builder": "nmslib_b200 host builder"},
+                           "index_builder": index_builder, "index_build": BUILD_INFO.get(WORKLOAD)},
                 "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": int(h_q.nbytes),
                         "d2h_bytes_per_step": int(nq * K * 8 + nq * 4)},
                 "gpu_launches": args.steps,
@@ -675,6 +857,7 @@ def main():
                              "distances_per_launch": n_dist},
                 "cpu_baseline": cpu,
                 "clocks": clk.summary(),
+                "parity": parity,
                 "sweep": sweep,
                 "launch": {"autotuned_shape": {"warps_per_block": best_shape[0], "rows_per_group": best_shape[1],
                                                "visited_hash_log2": best_shape[2], "stage_rows": best_shape[3]},
@@ -686,6 +869,54 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def full_size_parity(index, path, queries, space, efs):
+    """The engine's lists against the reference's knnQueryBatch on the same index file and
+    queries, at each efSearch of `efs` (the whole batch, all host threads)."""
+    ref = reference_module_or_none()
+    if ref is None:
+        return {"unavailable": "reference module not built (oracle/_ref)"}
+    r = ref.init(method="hnsw", space=space)
+    r.loadIndex(path)
+    out = {}
+    for ef in efs:
+        index.setQueryTimeParams({"efSearch": ef})
+        ids, dd, cnt = index.knnQueryBatchArrays(queries, K)
+        r.setQueryTimeParams({"efSearch": ef})
+        ri, rd, rc = reference_arrays(r, queries, K, os.cpu_count() or 1)
+        out[f"ef{ef}"] = list_parity(ids, dd, cnt, ri, rd, rc)
+        log(f"[bench] parity ef={ef}: {out[f'ef{ef}']}")
+    index.setQueryTimeParams({"efSearch": HEADLINE_EF})
+    return out
+
+
+def c1_parity(device):
+    """The plain small configuration: 10K x 128 Gaussian mixture, l2, M 16, efConstruction 200,
+    built by the reference's createIndex; efSearch 100, k 10, 1K queries. The engine against the
+    reference's knnQueryBatch on that file, and recall@10 against exact float64 neighbours."""
+    import nmslib_b200 as nmslib
+    name = "c1_gauss10k_d128_l2"
+    base, queries, space, m = workload_data(name)
+    path = ensure_index(name, base, space, m, 0, 1)
+    ref = reference_module_or_none()
+    if path is None or ref is None:
+        return {"unavailable": "reference module not built (oracle/_ref)"}
+    idx = nmslib.init(method="hnsw", space=space, device=device)
+    idx.loadIndex(path)
+    idx.setQueryTimeParams({"efSearch": 100})
+    ids, dd, cnt = idx.knnQueryBatchArrays(queries, K)
+    r = ref.init(method="hnsw", space=space)
+    r.loadIndex(path)
+    r.setQueryTimeParams({"efSearch": 100})
+    ri, rd, rc = reference_arrays(r, queries, K, os.cpu_count() or 1)
+    _, kth, _ = ground_truth(base, queries, K)
+    out = list_parity(ids, dd, cnt, ri, rd, rc)
+    out.update({"efSearch": 100, "k": K, "recall@10": round(recall_at_k(dd, cnt, kth, K), 4),
+                "recall@10_reference": round(recall_at_k(rd, rc, kth, K), 4),
+                "index_build": BUILD_INFO.get(name)})
+    log(f"[bench] c1 parity: {out}")
+    return out
 
 
 if __name__ == "__main__":

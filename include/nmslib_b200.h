@@ -149,6 +149,11 @@ typedef struct nmsg_launch_config {
                                 asynchronous copies (1..64); -1 = use the register gather */
   int32_t visited_hash_log2; /* per-query shared-memory visited table of 2^x ids (8..14);
                                 -1 = visited set in HBM only */
+  int32_t plain_slots;       /* one-query-per-block kernel: query slots (visited sets) its blocks
+                                share; 0 = one per resident block. With fewer slots than resident
+                                blocks, a block that finds no free slot in one bounded pass gives up:
+                                its query returns nothing and the call fails with NMSG_ERR_TIMEOUT
+                                (a way to exercise that bounded wait) */
 } nmsg_launch_config;
 
 /* Set (cfg != NULL) or reset to automatic (cfg == NULL) the launch shape used by later
@@ -156,17 +161,19 @@ typedef struct nmsg_launch_config {
 NMSG_API int nmsg_set_launch_config(nmsg_index* index, const nmsg_launch_config* cfg);
 
 /* nmsg_knn_batch for callers that cannot allocate device memory — no counterpart in the
- * reference (NMSLIB is CPU-only). Some callers must not call cudaMalloc at query time: code
- * running inside a stream capture that has to stay allocation-free, real-time serving threads
- * that may not touch the allocator, and processes whose device memory is reserved up front by
- * another pool. This entry point allocates nothing: queries, ids, dists and counts are caller-
- * owned DEVICE buffers (row stride kmax), k is uniform and ef/algoType are the handle's, and all
- * per-call scratch comes from one fixed 32 MiB device array that every GPU loading this library
- * holds until the process exits. It fails with NMSG_ERR_CAPACITY when the index needs more than
- * that for even one query slot (one slot needs round_up(n, 16) + 1 bytes, plus
- * 8 * min(n + 1, 131072) bytes when SearchOld runs). The first call on a device looks up the
- * array's device address; make it before any stream capture. Calls share the array: calls that
- * overlap on the GPU race with each other. Returns after the search has finished. */
+ * reference (NMSLIB is CPU-only). Some callers must not call cudaMalloc at query time: real-time
+ * serving threads that may not enter the allocator (its latency is unbounded), processes whose
+ * device memory is reserved up front by another framework's pool, and plug-ins inside such an
+ * engine. This entry point allocates nothing: queries, ids, dists and counts are caller-owned
+ * DEVICE buffers (row stride kmax), k is uniform and ef/algoType are the handle's, and all per-call
+ * scratch comes from one fixed 32 MiB device array that every GPU loading this library holds until
+ * the process exits. One query slot needs round_up(n, 16) + 1 bytes (plus 8 * min(n + 1, 131072)
+ * bytes when SearchOld runs), so the array bounds the queries in flight (33 at n = 1M) and the call
+ * fails with NMSG_ERR_CAPACITY when not even one slot fits. The first call on a device looks up the
+ * array's device address; make it before any stream capture. Calls share the array, which keeps
+ * the last call's contents (a call with the previous call's slot layout reuses its visited-set
+ * epochs; any other call clears what it uses): calls that overlap on the GPU race with each other.
+ * Returns after the search has finished. */
 NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* index, const float* queries, int64_t nq, int32_t dim, int32_t k,
                                     int32_t kmax, int32_t* ids, float* dists, int32_t* counts, void* stream);
 

@@ -89,7 +89,7 @@ struct SmemLayout {
     id_off = key_off + HALVES * BM * LIST_STRIDE * 4;
     nrm_off = id_off + HALVES * BM * LIST_STRIDE * 4;  // per epilogue warp: its 128 columns' |x|^2
     bar_off = (nrm_off + EPI_WARPS * (BN / HALVES) * 4 + 7) & ~7;
-    total = bar_off + 8 * (2 * 4 + 2 + 4) + 16;
+    total = bar_off + 8 * (2 * 4 + 2 + 4 + 1) + 16;
   }
 };
 
@@ -179,7 +179,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* q_empty = bars + 9;
   uint64_t* acc_full = bars + 10;   // [2]
   uint64_t* acc_empty = bars + 12;  // [2]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 14);
+  uint64_t* mma_drain = bars + 14;  // the MMA thread's last commit, waited on before teardown
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 15);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n_items = a.q_blocks * a.n_chunks;
   const int stages = a.stages;
@@ -195,6 +196,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&acc_full[i], 1);
       mbar_init(&acc_empty[i], EPI_WARPS);  // one arrival per epilogue warp
     }
+    mbar_init(mma_drain, 1);
     fence_barrier_init();
   }
   if (warp == 0) tmem_alloc(tmem_slot, 512);
@@ -205,12 +207,16 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == EPI_WARPS) {
     // ------------------------------------------------ TMA producer
+    // A load is issued only after its slot's empty barrier completed. After a failed wait nothing
+    // more is issued, and before the role ends it waits (bounded) for the last load armed on each
+    // slot, so no TMA write into shared memory is in flight when the CTA tears down.
     if (lane == 0) {
       prefetch_tmap(&tmq);
       prefetch_tmap(&tmx);
       int stage = 0;
       uint32_t xphase = 0, qphase = 0;
       int prev_qb = -1;
+      int x_armed = 0, q_armed = 0;  // loads armed on x_full (all stages) and on q_full
       // items are chunk-major: the CTAs running at the same time read the same base chunk, which
       // stays in L2 while every query block passes over it. The query block is loaded only when
       // it differs from the previous item's (for batches of <= 128 queries, once per CTA).
@@ -225,6 +231,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           mbar_arrive_expect_tx(q_full, a.kb * Q_BLOCK_BYTES);
           for (int kb = 0; kb < a.kb; ++kb) tma_load_2d(sq + kb * Q_BLOCK_BYTES, &tmq, q_full, kb * BK, qb * BM);
+          ++q_armed;
           prev_qb = qb;
         }
         const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
@@ -235,6 +242,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!ok) break;
             mbar_arrive_expect_tx(&x_full[stage], X_STAGE_BYTES);
             tma_load_2d(sx + stage * X_STAGE_BYTES, &tmx, &x_full[stage], kb * BK, t * BN);
+            ++x_armed;
             if (++stage == stages) {
               stage = 0;
               xphase ^= 1;
@@ -242,21 +250,34 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
       }
+      // drain: the c-th arming of a barrier (from 0) completes its phase c, so the last load on
+      // slot s has parity (arms(s) - 1) & 1; earlier loads on s completed before its reuse
+      for (int s = 0; s < stages; ++s) {
+        const int arms = x_armed / stages + (s < x_armed % stages ? 1 : 0);
+        if (arms > 0 && !mbar_wait(&x_full[s], (uint32_t)((arms - 1) & 1))) ok = false;
+      }
+      if (q_armed > 0 && !mbar_wait(q_full, (uint32_t)((q_armed - 1) & 1))) ok = false;
     }
   } else if (warp == EPI_WARPS + 1) {
     // ------------------------------------------------ MMA issuer
+    // No MMA and no commit is issued after a failed wait. Every MMA reads operands whose full
+    // barrier completed, and before the role ends one last commit (only if an MMA was ever issued)
+    // is waited on (bounded), so no tensor-core work is in flight at the final barrier and TMEM
+    // deallocation.
     if (lane == 0) {
       const uint32_t idesc = idesc_bf16_f32(BM, BN);
       int stage = 0;
       uint32_t xphase = 0, qphase = 0;
       uint32_t accphase[2] = {0, 0};
       int tcount = 0, prev_qb = -1;
+      bool issued = false;  // some MMA was issued by this thread
       for (int item = next_active_item<MODE>(a, blockIdx.x, n_items); item < n_items && ok;) {
         const int next = next_active_item<MODE>(a, item + gridDim.x, n_items);
         const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
         if (qb != prev_qb) {
           ok = mbar_wait(q_full, qphase);
           qphase ^= 1;
+          if (!ok) break;
           tc_fence_after();
           prev_qb = qb;
         }
@@ -265,26 +286,35 @@ __global__ void __launch_bounds__(kThreads, 1)
           const int buf = tcount & 1;
           ok = mbar_wait(&acc_empty[buf], accphase[buf] ^ 1);
           accphase[buf] ^= 1;
+          if (!ok) break;
           tc_fence_after();
           const uint32_t dcol = tmem + buf * BN;
-          for (int kb = 0; kb < a.kb && ok; ++kb) {
+          for (int kb = 0; kb < a.kb; ++kb) {
             ok = mbar_wait(&x_full[stage], xphase);
+            if (!ok) break;
             tc_fence_after();
             const uint32_t qa = smem_u32(sq + kb * Q_BLOCK_BYTES), xa = smem_u32(sx + stage * X_STAGE_BYTES);
 #pragma unroll
             for (int k = 0; k < BK / 16; ++k)
               umma_bf16(dcol, smem_desc_sw128(qa + 32 * k), smem_desc_sw128(xa + 32 * k), idesc, kb > 0 || k > 0);
+            issued = true;
             umma_commit(&x_empty[stage]);
             if (++stage == stages) {
               stage = 0;
               xphase ^= 1;
             }
           }
+          if (!ok) break;
           umma_commit(&acc_full[buf]);
         }
+        if (!ok) break;
         // the query block's buffer is free for the next one once these MMAs complete
-        if (next < n_items && next % a.q_blocks != qb) umma_commit(q_empty);
+        if (issued && next < n_items && next % a.q_blocks != qb) umma_commit(q_empty);
         item = next;
+      }
+      if (issued) {
+        umma_commit(mma_drain);
+        if (!mbar_wait(mma_drain, 0)) ok = false;
       }
     }
   } else {

@@ -262,9 +262,10 @@ int nmsg_last_device_status(const nmsg_index* h) { return h ? h->last_status : N
 
 int nmsg_set_launch_config(nmsg_index* h, const nmsg_launch_config* cfg) {
   if (!h) return fail(NMSG_ERR_BAD_ARG, "null index");
-  nmsg_launch_config c{0, 0, 0, 0};
+  nmsg_launch_config c{0, 0, 0, 0, 0};
   if (cfg) {
     c = *cfg;
+    if (c.plain_slots < 0) return fail(NMSG_ERR_BAD_ARG, "plain_slots must be >= 0");
     const int w = c.warps_per_block, r = c.rows_per_group, hl = c.visited_hash_log2, sr = c.stage_rows;
     if (!(w == 0 || w == 1 || w == 2 || w == 4)) return fail(NMSG_ERR_BAD_ARG, "warps_per_block must be 0, 1, 2 or 4");
     if (!(r == 0 || r == 1 || r == 2 || r == 4)) return fail(NMSG_ERR_BAD_ARG, "rows_per_group must be 0, 1, 2 or 4");
@@ -345,7 +346,9 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
   a.warp_smem = plan.warp_smem;
   const int gather = plan.gather, wpb = plan.wpb, bps = plan.blocks_per_sm;
   const int blocks = plain ? 0 : bps * h->num_sms;
-  const int slots = plain ? bps * h->num_sms : blocks * wpb;
+  const int slots = plain ? (h->cfg.plain_slots > 0 ? std::min(h->cfg.plain_slots, bps * h->num_sms)
+                                                   : bps * h->num_sms)
+                          : blocks * wpb;
   // scratch
   const int64_t vpitch = ((d.n + 15) / 16) * 16;
   if (slots > h->slots || (int64_t)h->visited.bytes < (int64_t)slots * vpitch) {

@@ -1,18 +1,28 @@
 // nmsg_knn_batch_noalloc: the batch search for callers that must not allocate device memory.
 //
-// Some callers cannot call cudaMalloc at query time: code running inside a CUDA stream capture
-// that must stay allocation-free, real-time serving threads that may not touch the allocator,
-// and hosts whose device memory is fully reserved up front by another framework's pool. For
-// them this entry point runs the same persistent search kernel as nmsg_knn_batch with device
-// pointers, but takes every piece of per-call scratch (work counter, status word, visited-set
-// epoch bytes, SearchOld candidate heaps) from one file-scope device array of fixed size
-// instead of the handle's grow-on-demand buffers.
+// Some callers cannot call cudaMalloc at query time: real-time serving threads that may not
+// enter the allocator (cudaMalloc can block on device-wide synchronisation and locks, so its
+// latency is unbounded), hosts whose device memory is fully reserved up front by another
+// framework's pool (a new allocation would fail or evict that pool's memory), and plug-ins
+// running inside such an engine. For them this entry point runs the same persistent search kernel
+// as nmsg_knn_batch with device pointers, but takes every piece of per-call scratch (work
+// counter, status word, per-slot epochs, visited-set epoch bytes, SearchOld candidate heaps) from
+// one file-scope device array of fixed size instead of the handle's grow-on-demand buffers.
 //
 // The array, kNoAllocScratchBytes (32 MiB), exists on every device that loads this library, for
 // the life of the process. Its host-side name is only a stand-in for the device symbol: the
 // device address is obtained once per device with cudaGetSymbolAddress (with that device
-// current) on the first call that runs on the device, and passed to the kernel. Make that first
-// call before any stream capture that should contain this entry point.
+// current) on the first call that runs on the device, and passed to the kernel; that first call
+// should come before any stream capture. One query slot needs round_up(n, 16) + 1 bytes (plus
+// the SearchOld heaps when they run), so the array limits how many queries run at once: at
+// n = 1M it holds 33 slots, i.e. 33 query warps in flight instead of the thousands the
+// allocating entry point runs, and throughput drops accordingly.
+//
+// Calls share the array and it keeps the last call's contents. The epoch bytes stay valid across
+// calls that use the same slot layout (each query takes the next epoch of its slot, as the
+// reference's VisitedList does), so such a call clears only its work counter and status word; a
+// call with a different layout (another index, or another ef / k that changes the slot count)
+// clears every byte it uses first. Calls that overlap on the GPU race on the array.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,6 +46,16 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 std::mutex g_scratch_mu;
 void* g_scratch_addr[kMaxDevices] = {};
+
+// Slot layout of the last call on each device (host-side record): a call with the same layout
+// keeps the epoch and visited bytes the previous one left, which are consistent by construction.
+struct ScratchLayout {
+  int64_t slots = -1, vpitch = -1, old_cap = -1;
+  bool operator==(const ScratchLayout& o) const {
+    return slots == o.slots && vpitch == o.vpitch && old_cap == o.old_cap;
+  }
+};
+ScratchLayout g_last_layout[kMaxDevices];
 
 // Device address of g_noalloc_scratch on `device` (which must be current), looked up once.
 int scratch_address(int device, void** out) {
@@ -162,9 +182,24 @@ extern "C" NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* h, const float* queri
   a.num_slots = (int)slots;
   const size_t used = (size_t)(reinterpret_cast<char*>(a.old_heap + slots * old_cap) - p);
 
-  // every call starts from zeroed counters, epochs and visited bytes
-  cudaError_t e = cudaMemsetAsync(base, 0, used, st);
+  // the work counter and status word start at zero; epochs and visited bytes too unless the
+  // previous call on this device used the same layout
+  ScratchLayout layout;
+  layout.slots = slots;
+  layout.vpitch = vpitch;
+  layout.old_cap = old_cap;
+  bool same_layout;
+  {
+    std::lock_guard<std::mutex> lk2(g_scratch_mu);
+    same_layout = g_last_layout[h->device] == layout;
+    g_last_layout[h->device] = ScratchLayout();  // unknown until the clear below is queued
+  }
+  cudaError_t e = cudaMemsetAsync(base, 0, same_layout ? 256 : used, st);
   if (e != cudaSuccess) return cuda_error(e, "clear no-alloc scratch");
+  {
+    std::lock_guard<std::mutex> lk2(g_scratch_mu);
+    g_last_layout[h->device] = layout;
+  }
   rc = launch_search(a, false, gather, old, blocks, wpb, stream);
   if (rc != 0) return cuda_error((cudaError_t)rc, "no-alloc search kernel launch");
   int32_t status = 0;

@@ -620,6 +620,15 @@ void* oracle_sift_load(const char* graph_path, const char* data_path) {
   }
   uint64_t qty = 0;
   dat.read(reinterpret_cast<char*>(&qty), 8);
+  // every object takes 8 (length) + 16 (header) + 128 (vector) + 4 (norm) bytes: a count the
+  // file cannot hold is rejected before anything is sized from it
+  dat.seekg(0, std::ios::end);
+  const uint64_t fsize = dat ? (uint64_t)dat.tellg() : 0;
+  dat.seekg(8, std::ios::beg);
+  if (!dat || fsize < 8 || qty > (fsize - 8) / (8 + 16 + kSiftDim + 4)) {
+    g_err = "objects file: object count " + std::to_string(qty) + " does not fit the file";
+    return nullptr;
+  }
   ix->vecs.resize(qty * kSiftDim);
   ix->norms.resize(qty);
   ix->obj_ids.resize(qty);

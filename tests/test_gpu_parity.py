@@ -215,3 +215,29 @@ def test_concurrent_launches_with_different_shared_memory():
     for t in threads:
         t.join()
     assert not errors, errors
+
+
+def test_plain_kernel_slot_wait_gives_up_with_timeout():
+    """The one-query-per-block kernel takes a visited-set slot with one bounded pass over the slot
+    locks. With a single slot for a whole batch, the blocks that find it taken give up: the call
+    reports NMSG_ERR_TIMEOUT (no spin, no fault), and the next call with the normal slot count is
+    clean and exact."""
+    from nmslib_b200 import _capi
+    name = "c1_l2_d128"
+    q = load_golden(name)["queries"]
+    idx = _gpu_index(name)
+    idx.setQueryTimeParams({"efSearch": 100})
+    idx.setLaunchConfig(plain_slots=1)
+    try:
+        with pytest.raises(RuntimeError, match=f"status {_capi.ERR_TIMEOUT}"):
+            idx.knnQueryBatchArrays(q, 10, plain=True)
+        assert _capi.load().nmsg_last_device_status(idx._h) == _capi.ERR_TIMEOUT
+    finally:
+        idx.setLaunchConfig()
+    oi, od, oc, _ = _oracle(name).search(q, k=10, ef=100)
+    for plain in (True, False):
+        ids, d, cnt = idx.knnQueryBatchArrays(q, 10, plain=plain)
+        np.testing.assert_array_equal(cnt, oc)
+        np.testing.assert_array_equal(ids, oi)
+        np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
+    assert _capi.load().nmsg_last_device_status(idx._h) == 0

@@ -86,3 +86,8 @@ def test_sift_loader_rejects_mismatched_files(tmp_path):
         OracleSiftIndex(os.path.join(HERE, "sift_u8_tiny.hnsw"), str(bad))
     with pytest.raises(ValueError, match="not a regular index"):
         OracleSiftIndex(os.path.join(HERE, "c1_l2_d128.hnsw"), os.path.join(HERE, "sift_u8_tiny.hnsw.dat"))
+    # a count far beyond what the file holds is refused before anything is sized from it
+    huge = tmp_path / "huge.dat"
+    huge.write_bytes(np.array([1 << 60], np.uint64).tobytes() + b"\0" * 200)
+    with pytest.raises(ValueError, match="does not fit the file"):
+        OracleSiftIndex(os.path.join(HERE, "sift_u8_tiny.hnsw"), str(huge))
