@@ -54,7 +54,11 @@ enum nmsg_status {
 /* Space names of nmslib.init(space=...): 'l2', 'cosinesimil', 'negdotprod', 'l1', 'linf'. The
  * last two are the optimized index's distance codes 5 and 6 (L1NormSIMD / LInfNormSIMD,
  * similarity_search/src/method/hnsw.cc:83-89, src/distcomp_lp.cc:77-251). */
-enum nmsg_space { NMSG_SPACE_L2 = 0, NMSG_SPACE_COSINE = 1, NMSG_SPACE_NEGDOT = 2, NMSG_SPACE_L1 = 3, NMSG_SPACE_LINF = 4 };
+enum nmsg_space { NMSG_SPACE_L2 = 0, NMSG_SPACE_COSINE = 1, NMSG_SPACE_NEGDOT = 2, NMSG_SPACE_L1 = 3, NMSG_SPACE_LINF = 4,
+                  /* 'l2sqr_sift' with data_type DENSE_UINT8_VECTOR and dtype INT: 128 uint8 values per
+                   * object, int squared L2 (similarity_search/src/space/space_l2sqr_sift.cc,
+                   * src/distcomp_l2sqr_sift.cc:40-50); indices in the regular format + objects file */
+                  NMSG_SPACE_L2SQR_SIFT = 5 };
 
 /* algoType of setQueryTimeParams (hnsw.cc:486-497): hybrid uses SearchOld when ef >= 1000. */
 enum nmsg_algo { NMSG_ALGO_HYBRID = 0, NMSG_ALGO_OLD = 1, NMSG_ALGO_V1MERGE = 2 };
@@ -88,6 +92,20 @@ typedef struct nmsg_index_info {
  * as IndexWrapper::loadIndex does through ResetQueryTimeParams (nmslib.cc:112). */
 NMSG_API int nmsg_index_load(const char* path, int space, int device, nmsg_index** out);
 
+/* Load an index whose vectors live in a separate objects file, like IndexWrapper::loadIndex(path,
+ * load_data=True) (python_bindings/nmslib.cc:98-113): the objects from `data_path` (the
+ * reference's `path + ".dat"`, Space::ReadObjectVectorFromBinData, space.cc) and the regular graph
+ * file from `path` (Hnsw::LoadRegularIndexBin, similarity_search/src/method/hnsw.cc:943-991).
+ * Space NMSG_SPACE_L2SQR_SIFT only (the reference has no optimized layout for it). Every count,
+ * id and level is validated before the upload. ef is 20 and algo hybrid after the load. */
+NMSG_API int nmsg_index_load_with_data(const char* path, const char* data_path, int space, int device,
+                                       nmsg_index** out);
+
+/* saveIndex(path, save_data=True) for an index loaded with nmsg_index_load_with_data
+ * (nmslib.cc:115-125): the regular graph file (Hnsw::SaveRegularIndexBin, hnsw.cc:810-842) and the
+ * objects file (Space::WriteObjectVectorBinData, space.cc); byte-identical to the reference's. */
+NMSG_API int nmsg_index_save_with_data(const nmsg_index* index, const char* path, const char* data_path);
+
 /* Write the loaded index back in the reference's optimized format (hnsw.cc:774-806). */
 NMSG_API int nmsg_index_save(const nmsg_index* index, const char* path);
 
@@ -113,6 +131,15 @@ NMSG_API int nmsg_set_query_params(nmsg_index* index, int ef, int algo);
 NMSG_API int nmsg_knn_batch(nmsg_index* index, const float* queries, int64_t nq, int32_t dim, int32_t k,
                    const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids,
                    float* dists, int32_t* counts, int64_t* stats, uint32_t flags, void* stream);
+
+/* nmsg_knn_batch for l2sqr_sift indices: IndexWrapper<int>::knnQueryBatch over
+ * DENSE_UINT8_VECTOR queries (nmslib.cc:142-168, :258-272: each query row becomes an object
+ * with its int sum of squares) -> the generic Hnsw searches (hnsw.cc:1078-1290, the same steps as
+ * the optimized ones). queries: nq x 128 uint8; dists: int32 squared L2 (INT32_MAX padding);
+ * every other argument as nmsg_knn_batch. */
+NMSG_API int nmsg_knn_batch_u8(nmsg_index* index, const uint8_t* queries, int64_t nq, int32_t dim, int32_t k,
+                               const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids,
+                               int32_t* dists, int32_t* counts, int64_t* stats, uint32_t flags, void* stream);
 
 /* Build an HNSW index on the host and write it in the optimized format, like
  * IndexWrapper::createIndex + saveIndex (python_bindings/nmslib.cc:89-96, :115-125)

@@ -292,7 +292,150 @@ class FloatIndex:
         return self.knnQueryBatch(v, k)[0]
 
 
+class IntIndex(FloatIndex):
+    """Mirror of ``IndexWrapper<int>`` for method='hnsw', space='l2sqr_sift' over
+    DENSE_UINT8_VECTOR data (128 uint8 values per object, int squared L2 distances,
+    similarity_search/src/space/space_l2sqr_sift.cc). The reference saves such an index only in the
+    regular format with a separate objects file, so ``loadIndex`` needs ``load_data=True`` (or
+    rows added first with ``addDataPointBatch``) and ``saveIndex`` writes both files with
+    ``save_data=True``. Building is the reference's job (``createIndex`` is not offered)."""
+
+    def __init__(self, method, space, space_params, data_type, dtype, device=0):
+        if method not in METHODS:
+            raise ValueError(f"The B200 engine implements method 'hnsw' only, got {method!r}")
+        if space != "l2sqr_sift":
+            raise ValueError(f"The B200 engine implements integer distances for space 'l2sqr_sift' only, got {space!r}")
+        if _load_params(space_params):
+            raise RuntimeError("Unknown parameters found!")
+        if data_type != DataType.DENSE_UINT8_VECTOR:
+            raise ValueError(f"The space type {space} is not compatible with the type {DataType(data_type).name}!")
+        self.method, self.space, self.device = method, space, int(device)
+        self.dataType, self.distType = DataType(data_type), DistType(dtype)
+        self._h = ctypes.c_void_p()
+        self._info = None
+        self._data = []
+        self._ids = []
+
+    def __repr__(self):
+        return f"<nmslib_b200.IntIndex method={self.method} space={self.space} n={len(self)}>"
+
+    def _queries(self, input):
+        """py::array_t<uint8_t, c_style | forcecast> (nmslib.cc:258-272): 2-D rows of uint8."""
+        if isinstance(input, list):
+            input = np.stack([np.asarray(r).reshape(-1) for r in input]) if input else np.zeros((0, 128))
+        q = np.ascontiguousarray(np.asarray(input).astype(np.uint8, copy=False))
+        if q.ndim != 2:
+            raise RuntimeError("data must be a 2d array")
+        return q
+
+    def addDataPointBatch(self, data, ids=None):
+        x = self._queries(data)
+        if x.shape[1] != 128:
+            raise RuntimeError(f"Bug or internal error, SIFT vectors dim {x.shape[1]} isn't == 128")
+        start = sum(len(d) for d in self._data)
+        idv = np.arange(start, start + len(x), dtype=np.int64) if ids is None else np.asarray(ids, np.int64).reshape(-1)
+        if len(idv) != len(x):
+            raise ValueError("ids must have one entry per row")
+        self._data.append(x)
+        self._ids.append(idv)
+        return len(x)
+
+    def addDataPoint(self, id, data):
+        self.addDataPointBatch(np.asarray(data).reshape(1, -1), ids=[id])
+        return sum(len(d) for d in self._data) - 1
+
+    def createIndex(self, index_params=None, print_progress=False):
+        raise RuntimeError("the B200 engine loads l2sqr_sift indices built by the reference's createIndex; "
+                           "it does not build them")
+
+    def _objects_file(self, path):
+        """Objects added with addDataPointBatch written in the reference's objects-file format
+        (u64 count; per object u64 length, i32 id, i32 label -1, u64 132, 128 values, i32 norm)."""
+        data = np.concatenate(self._data)
+        ids = np.concatenate(self._ids).astype(np.int32)
+        norms = (data.astype(np.int64) ** 2).sum(1).astype(np.int32)
+        rec = np.zeros(len(data), dtype=[("len", "<u8"), ("id", "<i4"), ("label", "<i4"), ("dlen", "<u8"),
+                                         ("v", "u1", 128), ("norm", "<i4")])
+        rec["len"], rec["id"], rec["label"], rec["dlen"], rec["v"], rec["norm"] = 148, ids, -1, 132, data, norms
+        with open(path, "wb") as f:
+            f.write(np.uint64(len(data)).tobytes())
+            f.write(rec.tobytes())
+
+    def loadIndex(self, filename, load_data=False):
+        """IndexWrapper::loadIndex (nmslib.cc:98-113): with load_data the objects come from
+        ``filename + '.dat'``, else from rows added before; then the regular graph file."""
+        lib = _capi.load()
+        h = ctypes.c_void_p()
+        if load_data:
+            rc = lib.nmsg_index_load_with_data(os.fsencode(filename), os.fsencode(filename + ".dat"),
+                                               _capi.SPACE_L2SQR_SIFT, self.device, ctypes.byref(h))
+        else:
+            import tempfile
+            with tempfile.TemporaryDirectory() as tmp:
+                dat = os.path.join(tmp, "objects.dat")
+                if self._data:
+                    self._objects_file(dat)
+                else:
+                    with open(dat, "wb") as f:
+                        f.write(np.uint64(0).tobytes())
+                rc = lib.nmsg_index_load_with_data(os.fsencode(filename), os.fsencode(dat), _capi.SPACE_L2SQR_SIFT,
+                                                   self.device, ctypes.byref(h))
+        _capi.check(rc)
+        if self._h:
+            lib.nmsg_index_free(self._h)
+        self._h = h
+        self._refresh_info()
+
+    def saveIndex(self, filename, save_data=False):
+        """saveIndex (nmslib.cc:115-125): the regular graph file, and with save_data the objects
+        file ``filename + '.dat'``."""
+        h = self._require()
+        import tempfile
+        with tempfile.TemporaryDirectory() as tmp:
+            dat = filename + ".dat" if save_data else os.path.join(tmp, "objects.dat")
+            _capi.check(_capi.load().nmsg_index_save_with_data(h, os.fsencode(filename), os.fsencode(dat)))
+
+    def knnQueryBatchArrays(self, queries, k=10, ef=None, plain=False, stats=False):
+        """Batch search returning dense arrays: (ids [nq, kmax] int32, -1 padding; dists
+        [nq, kmax] int32, INT32_MAX padding; counts [nq][, stats [nq, 4]])."""
+        h = self._require()
+        q = self._queries(queries)
+        nq = q.shape[0]
+        k_arr = None
+        if np.ndim(k):
+            k_arr = np.ascontiguousarray(np.asarray(k, dtype=np.int32).reshape(-1))
+            if k_arr.shape[0] != nq:
+                raise ValueError("per-query k must have one entry per query")
+            kmax = int(k_arr.max()) if nq else 1
+        else:
+            kmax = int(k)
+        ef_arr = None
+        if ef is not None:
+            ef_arr = np.ascontiguousarray(np.broadcast_to(np.asarray(ef, dtype=np.int32), (nq,)))
+        kmax = max(kmax, 1)
+        ids = np.empty((nq, kmax), np.int32)
+        dists = np.empty((nq, kmax), np.int32)
+        counts = np.empty(nq, np.int32)
+        st = np.empty((nq, 4), np.int64) if stats else None
+        ptr = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        flags = _capi.FLAG_PLAIN_KERNEL if plain else 0
+        dim = q.shape[1] if nq else 128
+        _capi.check(_capi.load().nmsg_knn_batch_u8(h, ptr(q), nq, dim, 1 if k_arr is not None else kmax, ptr(k_arr),
+                                                   ptr(ef_arr), kmax, ptr(ids), ptr(dists), ptr(counts), ptr(st),
+                                                   flags, None))
+        return (ids, dists, counts, st) if stats else (ids, dists, counts)
+
+    def knnQuery(self, vector, k=10):
+        return self.knnQueryBatch(np.asarray(vector).reshape(1, -1), k)[0]
+
+    def bruteForceBatchArrays(self, queries, k=10, stats=False):
+        raise RuntimeError("brute force over l2sqr_sift indices is not supported")
+
+
 def init(space="cosinesimil", space_params=None, method="hnsw", data_type=DataType.DENSE_VECTOR,
          dtype=DistType.FLOAT, device=0):
-    """nmslib.init (python_bindings/nmslib.cc:470-510); ``device`` selects the CUDA device."""
+    """nmslib.init (python_bindings/nmslib.cc:470-510): DistType.FLOAT gives the float index,
+    DistType.INT the integer one (space 'l2sqr_sift'); ``device`` selects the CUDA device."""
+    if dtype == DistType.INT:
+        return IntIndex(method, space, space_params, data_type, dtype, device)
     return FloatIndex(method, space, space_params, data_type, dtype, device)

@@ -17,7 +17,7 @@ OK = 0
 ERR_BAD_FILE, ERR_UNSUPPORTED, ERR_BAD_ARG, ERR_OOM = -1, -2, -3, -4
 ERR_DEVICE, ERR_TIMEOUT, ERR_CORRUPT_GRAPH, ERR_CAPACITY = -5, -6, -7, -8
 
-SPACE_L2, SPACE_COSINE, SPACE_NEGDOT, SPACE_L1, SPACE_LINF = 0, 1, 2, 3, 4
+SPACE_L2, SPACE_COSINE, SPACE_NEGDOT, SPACE_L1, SPACE_LINF, SPACE_L2SQR_SIFT = 0, 1, 2, 3, 4, 5
 ALGO_HYBRID, ALGO_OLD, ALGO_V1MERGE = 0, 1, 2
 FLAG_DEVICE_PTRS, FLAG_PLAIN_KERNEL, FLAG_CUDA_GRAPH = 1, 2, 4
 
@@ -58,6 +58,13 @@ def load(path: str = LIB_PATH):
     lib.nmsg_index_load.restype = ctypes.c_int
     lib.nmsg_index_save.argtypes = [P, ctypes.c_char_p]
     lib.nmsg_index_save.restype = ctypes.c_int
+    lib.nmsg_index_load_with_data.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.POINTER(P)]
+    lib.nmsg_index_load_with_data.restype = ctypes.c_int
+    lib.nmsg_index_save_with_data.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
+    lib.nmsg_index_save_with_data.restype = ctypes.c_int
+    lib.nmsg_knn_batch_u8.argtypes = [P, P, I64, I32, I32, P, P, I32, P, P, P, P, U32, P]
+    lib.nmsg_knn_batch_u8.restype = ctypes.c_int
     lib.nmsg_index_free.argtypes = [P]
     lib.nmsg_index_free.restype = None
     lib.nmsg_index_info_get.argtypes = [P, ctypes.POINTER(IndexInfo)]

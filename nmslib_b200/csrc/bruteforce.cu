@@ -987,6 +987,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
                                             int32_t kmax, int32_t* ids, float* dists, int32_t* counts,
                                             int64_t* stats, uint32_t flags, void* stream) {
   if (!h) return bf_fail(NMSG_ERR_BAD_ARG, "Must call createIndex or loadIndex before this method");
+  if (h->host.sift) return bf_fail(NMSG_ERR_UNSUPPORTED, "brute force over l2sqr_sift indices is not supported");
   if (nq < 0 || k < 1 || kmax < k) return bf_fail(NMSG_ERR_BAD_ARG, "nq must be >= 0, k >= 1 and kmax >= k");
   if (k > CAND) return bf_fail(NMSG_ERR_UNSUPPORTED, "brute force supports k <= 32");
   if (nq > 0 && (!queries || !ids || !dists || !counts)) return bf_fail(NMSG_ERR_BAD_ARG, "null buffer");

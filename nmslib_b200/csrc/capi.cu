@@ -54,6 +54,7 @@ int upload_index(nmsg_index* h) {
   d.pitch = (hi.dim + 31) & ~31;
   d.n16 = hi.dim & ~15;
   d.n4 = hi.dim & ~3;
+  d.row_bytes = 4 * hi.dim;
   d.maxM = (int)hi.maxM;
   d.maxM0 = (int)hi.maxM0;
   d.l0_pitch = ((int)hi.maxM0 + 1 + 7) & ~7;
@@ -94,6 +95,63 @@ int upload_index(nmsg_index* h) {
   return NMSG_OK;
 }
 
+// l2sqr_sift index: 128-byte rows (the values only; the stored norms go to the device only if
+// some stored norm differs from the sum of squares of its values, else the kernel recomputes
+// them from the row it has read), the level-0 lists padded to l0_pitch, upper lists as CSR with
+// a stride of capu + 1.
+int upload_sift(nmsg_index* h) {
+  const HostIndex& hi = h->host;
+  DevIndex& d = h->dev;
+  d = DevIndex();
+  d.n = hi.n;
+  d.dim = kSiftDim;
+  d.pitch = kSiftDim / 4 + 4;  // shared-memory query: 128 values, the norm, padding to 16 bytes
+  d.row_bytes = kSiftRowBytes;
+  d.dist_type = kSiftL2;
+  if (hi.n == 0) return NMSG_OK;
+  d.maxM = (int)hi.capu;
+  d.maxM0 = (int)hi.cap0;
+  d.l0_pitch = ((int)hi.cap0 + 1 + 7) & ~7;
+  d.maxlevel = hi.maxlevel;
+  d.enterpoint = (int)hi.enterpoint;
+  const int64_t n = hi.n;
+  std::vector<int32_t> l0((size_t)n * d.l0_pitch, 0);
+  bool norms_match = true;
+  for (int64_t i = 0; i < n; ++i) {
+    const int32_t* lst = hi.sift_l0.data() + i * (hi.cap0 + 1);
+    std::memcpy(l0.data() + i * d.l0_pitch, lst, 4 * (1 + lst[0]));
+    const uint8_t* v = hi.sift_vecs.data() + i * kSiftDim;
+    int32_t s2 = 0;
+    for (int e = 0; e < kSiftDim; ++e) s2 += int32_t(v[e]) * int32_t(v[e]);
+    norms_match &= s2 == hi.sift_norms[i];
+  }
+  std::vector<int32_t> links = hi.up_links;
+  if (links.empty()) links.push_back(0);
+  NMSG_CUDA(h->vecs.ensure((size_t)n * kSiftDim, false), "cudaMalloc(vectors)");
+  NMSG_CUDA(h->l0.ensure(l0.size() * 4, false), "cudaMalloc(level-0 lists)");
+  NMSG_CUDA(h->up_off.ensure(n * 8, false), "cudaMalloc(upper offsets)");
+  NMSG_CUDA(h->up_links.ensure(links.size() * 4, false), "cudaMalloc(upper lists)");
+  NMSG_CUDA(h->ext_id.ensure(n * 4, false), "cudaMalloc(ids)");
+  NMSG_CUDA(cudaMemcpy(h->vecs.p, hi.sift_vecs.data(), (size_t)n * kSiftDim, cudaMemcpyHostToDevice), "upload vectors");
+  NMSG_CUDA(cudaMemcpy(h->l0.p, l0.data(), l0.size() * 4, cudaMemcpyHostToDevice), "upload lists");
+  NMSG_CUDA(cudaMemcpy(h->up_off.p, hi.up_off.data(), n * 8, cudaMemcpyHostToDevice), "upload offsets");
+  NMSG_CUDA(cudaMemcpy(h->up_links.p, links.data(), links.size() * 4, cudaMemcpyHostToDevice), "upload links");
+  NMSG_CUDA(cudaMemcpy(h->ext_id.p, hi.sift_ids.data(), n * 4, cudaMemcpyHostToDevice), "upload ids");
+  if (!norms_match) {
+    NMSG_CUDA(h->norms.ensure(n * 4, false), "cudaMalloc(norms)");
+    NMSG_CUDA(cudaMemcpy(h->norms.p, hi.sift_norms.data(), n * 4, cudaMemcpyHostToDevice), "upload norms");
+    d.norms = h->norms.as<int32_t>();
+  }
+  d.vecs_u8 = h->vecs.as<uint8_t>();
+  d.l0 = h->l0.as<int32_t>();
+  d.up_off = h->up_off.as<int64_t>();
+  d.up_links = h->up_links.as<int32_t>();
+  d.ext_id = h->ext_id.as<int32_t>();
+  h->resident_bytes = (int64_t)((size_t)n * kSiftDim + l0.size() * 4 + n * 12 + links.size() * 4 +
+                                (norms_match ? 0 : n * 4));
+  return NMSG_OK;
+}
+
 int space_matches(int space, int dist_type) {
   switch (space) {
     case NMSG_SPACE_L2: return dist_type == kL2Sqr16Ext || dist_type == kL2SqrExt;
@@ -121,7 +179,9 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
   // (4.10M q/s at 64 vs 3.47M for two register rows per 8-lane group), 4 rows at efSearch 256
   // (1.90M vs 1.64M), where the larger beam array leaves less shared memory per warp.
   p.stage_rows = 0;
-  if (d.dist_type == kL1 || d.dist_type == kLInf) {
+  if (d.dist_type == kSiftL2) {
+    p.gather = kSiftGather;  // the only kernels compiled with the uint8 distance
+  } else if (d.dist_type == kL1 || d.dist_type == kLInf) {
     p.gather = kLpGather;  // the only kernels compiled with the L1 / LInf distances
   } else if (cfg.stage_rows > 0) {
     p.gather = 0;
@@ -211,8 +271,56 @@ int nmsg_index_load(const char* path, int space, int device, nmsg_index** out) {
 
 int nmsg_index_save(const nmsg_index* h, const char* path) {
   if (!h || !path) return fail(NMSG_ERR_BAD_ARG, "null argument");
+  if (h->host.sift)
+    return fail(NMSG_ERR_BAD_ARG, "an l2sqr_sift index is saved with its objects file: nmsg_index_save_with_data");
   std::string err;
   int rc = write_index_file(path, h->host, err);
+  return rc == NMSG_OK ? rc : fail(rc, err);
+}
+
+int nmsg_index_load_with_data(const char* path, const char* data_path, int space, int device, nmsg_index** out) {
+  if (!out || !path || !data_path) return fail(NMSG_ERR_BAD_ARG, "null argument");
+  *out = nullptr;
+  if (space != NMSG_SPACE_L2SQR_SIFT)
+    return fail(NMSG_ERR_UNSUPPORTED, "loading with a data file is supported for the l2sqr_sift space only");
+  auto* h = new nmsg_index();
+  h->device = device;
+  h->space = space;
+  std::string err;
+  const int rc0 = read_sift_index(path, data_path, h->host, err);
+  if (rc0 != NMSG_OK) {
+    delete h;
+    return fail(rc0, err);
+  }
+  int ndev = 0;
+  cudaError_t ce = cudaGetDeviceCount(&ndev);
+  if (ce != cudaSuccess || ndev == 0) {
+    delete h;
+    return fail(NMSG_ERR_DEVICE, "no CUDA device is available");
+  }
+  if (device < 0 || device >= ndev) {
+    delete h;
+    return fail(NMSG_ERR_BAD_ARG, "device ordinal out of range");
+  }
+  int rc;
+  {
+    DeviceGuard g(device);
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+    rc = upload_sift(h);
+  }
+  if (rc != NMSG_OK) {
+    nmsg_index_free(h);
+    return rc;
+  }
+  *out = h;
+  return NMSG_OK;
+}
+
+int nmsg_index_save_with_data(const nmsg_index* h, const char* path, const char* data_path) {
+  if (!h || !path || !data_path) return fail(NMSG_ERR_BAD_ARG, "null argument");
+  if (!h->host.sift) return fail(NMSG_ERR_UNSUPPORTED, "saving with a data file is supported for l2sqr_sift indices only");
+  std::string err;
+  const int rc = write_sift_index(path, data_path, h->host, err);
   return rc == NMSG_OK ? rc : fail(rc, err);
 }
 
@@ -224,7 +332,7 @@ void nmsg_index_free(nmsg_index* h) {
     if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
     destroy_bruteforce(h->bf);
     h->bf = nullptr;
-    for (DevBuf* b : {&h->vecs, &h->l0, &h->up_off, &h->up_links, &h->ext_id, &h->visited, &h->epochs, &h->locks,
+    for (DevBuf* b : {&h->vecs, &h->norms, &h->l0, &h->up_off, &h->up_links, &h->ext_id, &h->visited, &h->epochs, &h->locks,
                       &h->old_heap, &h->counter, &h->status, &h->order, &h->kq, &h->efq, &h->q_stage,
                       &h->ids_stage, &h->dists_stage, &h->counts_stage, &h->stats_stage})
       b->release();
@@ -278,10 +386,17 @@ int nmsg_set_launch_config(nmsg_index* h, const nmsg_launch_config* cfg) {
   return NMSG_OK;
 }
 
-int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim, int32_t k,
-                   const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids, float* dists,
+}  // extern "C"
+
+namespace {
+
+// The batch search behind nmsg_knn_batch (float queries and distances) and nmsg_knn_batch_u8
+// (l2sqr_sift: uint8 queries, int distances).
+int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, int32_t dim, int32_t k,
+                   const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids, void* dists_v,
                    int32_t* counts, int64_t* stats, uint32_t flags, void* stream) {
-  if (!h) return fail(NMSG_ERR_BAD_ARG, "Must call createIndex or loadIndex before this method");
+  const float* queries = static_cast<const float*>(queries_v);
+  float* dists = static_cast<float*>(dists_v);
   if (nq < 0) return fail(NMSG_ERR_BAD_ARG, "negative query count");
   if (nq > 0 && (!queries || !ids || !dists || !counts)) return fail(NMSG_ERR_BAD_ARG, "null buffer");
   const bool dev_ptrs = flags & NMSG_DEVICE_PTRS;
@@ -315,7 +430,10 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
     } else {
       std::fill(counts, counts + nq, 0);
       std::fill(ids, ids + nq * kmax, -1);
-      std::fill(dists, dists + nq * kmax, __builtin_inff());
+      if (u8)
+        std::fill(static_cast<int32_t*>(dists_v), static_cast<int32_t*>(dists_v) + nq * kmax, 0x7fffffff);
+      else
+        std::fill(dists, dists + nq * kmax, __builtin_inff());
       if (stats) std::fill(stats, stats + nq * 4, 0);
     }
     return NMSG_OK;
@@ -331,6 +449,7 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
   std::memset(&a, 0, sizeof(a));  // padding too: the CUDA-graph cache compares argument bytes
   a.ix = d;
   a.nq = nq;
+  a.dists_int = u8 ? 1 : 0;
   a.k_default = k;
   a.ef_default = ef;
   a.algo = algo;
@@ -381,9 +500,12 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
   a.status = h->status.as<int32_t>();
 
   // inputs / outputs
-  const size_t qbytes = (size_t)nq * dim * 4, obytes = (size_t)nq * kmax * 4;
+  const size_t qbytes = (size_t)nq * dim * (u8 ? 1 : 4), obytes = (size_t)nq * kmax * 4;
   if (dev_ptrs) {
-    a.queries = queries;
+    if (u8)
+      a.queries_u8 = static_cast<const uint8_t*>(queries_v);
+    else
+      a.queries = queries;
     a.ids = ids;
     a.dists = dists;
     a.counts = counts;
@@ -394,8 +516,11 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
     NMSG_CUDA(h->dists_stage.ensure(obytes, false), "cudaMalloc(distance staging)");
     NMSG_CUDA(h->counts_stage.ensure((size_t)nq * 4, false), "cudaMalloc(count staging)");
     if (stats) NMSG_CUDA(h->stats_stage.ensure((size_t)nq * 32, false), "cudaMalloc(stats staging)");
-    NMSG_CUDA(cudaMemcpyAsync(h->q_stage.p, queries, qbytes, cudaMemcpyHostToDevice, st), "copy queries");
-    a.queries = h->q_stage.as<float>();
+    NMSG_CUDA(cudaMemcpyAsync(h->q_stage.p, queries_v, qbytes, cudaMemcpyHostToDevice, st), "copy queries");
+    if (u8)
+      a.queries_u8 = h->q_stage.as<uint8_t>();
+    else
+      a.queries = h->q_stage.as<float>();
     a.ids = h->ids_stage.as<int32_t>();
     a.dists = h->dists_stage.as<float>();
     a.counts = h->counts_stage.as<int32_t>();
@@ -462,7 +587,7 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
   if (dev_ptrs) return NMSG_OK;
   int32_t dstatus = 0;
   NMSG_CUDA(cudaMemcpyAsync(ids, a.ids, obytes, cudaMemcpyDeviceToHost, st), "copy ids");
-  NMSG_CUDA(cudaMemcpyAsync(dists, a.dists, obytes, cudaMemcpyDeviceToHost, st), "copy distances");
+  NMSG_CUDA(cudaMemcpyAsync(dists_v, a.dists, obytes, cudaMemcpyDeviceToHost, st), "copy distances");
   NMSG_CUDA(cudaMemcpyAsync(counts, a.counts, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
   if (stats) NMSG_CUDA(cudaMemcpyAsync(stats, a.stats, nq * 32, cudaMemcpyDeviceToHost, st), "copy stats");
   NMSG_CUDA(cudaMemcpyAsync(&dstatus, a.status, 4, cudaMemcpyDeviceToHost, st), "copy status");
@@ -470,6 +595,31 @@ int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim,
   h->last_status = dstatus;
   if (dstatus != 0) return fail(dstatus, "the search kernel reported a device-side error (status " + std::to_string(dstatus) + ")");
   return NMSG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nmsg_knn_batch(nmsg_index* h, const float* queries, int64_t nq, int32_t dim, int32_t k,
+                   const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids, float* dists,
+                   int32_t* counts, int64_t* stats, uint32_t flags, void* stream) {
+  if (!h) return fail(NMSG_ERR_BAD_ARG, "Must call createIndex or loadIndex before this method");
+  if (h->host.sift)
+    return fail(NMSG_ERR_BAD_ARG, "this index holds uint8 (l2sqr_sift) vectors: search it with nmsg_knn_batch_u8");
+  return knn_batch_impl(h, queries, false, nq, dim, k, k_per_q, ef_per_q, kmax, ids, dists, counts, stats, flags,
+                        stream);
+}
+
+int nmsg_knn_batch_u8(nmsg_index* h, const uint8_t* queries, int64_t nq, int32_t dim, int32_t k,
+                      const int32_t* k_per_q, const int32_t* ef_per_q, int32_t kmax, int32_t* ids, int32_t* dists,
+                      int32_t* counts, int64_t* stats, uint32_t flags, void* stream) {
+  if (!h) return fail(NMSG_ERR_BAD_ARG, "Must call createIndex or loadIndex before this method");
+  if (!h->host.sift) return fail(NMSG_ERR_BAD_ARG, "nmsg_knn_batch_u8 searches l2sqr_sift indices only");
+  if (h->host.n > 0 && nq > 0 && dim != kSiftDim)
+    return fail(NMSG_ERR_BAD_ARG, "query dimension " + std::to_string(dim) + " does not match the index dimension 128");
+  return knn_batch_impl(h, queries, true, nq, dim, k, k_per_q, ef_per_q, kmax, ids, dists, counts, stats, flags,
+                        stream);
 }
 
 }  // extern "C"

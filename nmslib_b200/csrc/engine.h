@@ -16,10 +16,17 @@
 namespace nmsg {
 
 // Optimized-index distance codes (similarity_search/include/method/hnsw.h:50-58).
-enum DistCode { kL2Sqr16Ext = 1, kL2SqrExt = 2, kNormCosine = 3, kNegDot = 4, kL1 = 5, kLInf = 6 };
+// kSiftL2 is the engine's own code for space l2sqr_sift (128 uint8 values per object, int
+// distance; similarity_search/src/distcomp_l2sqr_sift.cc:40-50), whose indices exist only in the
+// regular format: it is not a reference DistFuncType and never appears in an optimized file.
+enum DistCode { kL2Sqr16Ext = 1, kL2SqrExt = 2, kNormCosine = 3, kNegDot = 4, kL1 = 5, kLInf = 6, kSiftL2 = 7 };
 // Gather code of the kernels compiled for L1 / LInf (one row per 8-lane group in registers);
 // 0 = rows staged in shared memory, 1 / 2 / 4 = register rows per group for the other codes.
 constexpr int kLpGather = 3;
+// Gather code of the kernels compiled for l2sqr_sift rows (one 128-byte row per 4-lane group).
+constexpr int kSiftGather = 5;
+constexpr int kSiftDim = 128;
+constexpr int kSiftRowBytes = kSiftDim + 4;  // the reference's object payload: values + int norm
 
 // The index as read from an optimized HNSW file, in host memory.
 // File layout (similarity_search/src/method/hnsw.cc:774-806):
@@ -42,6 +49,16 @@ struct HostIndex {
   std::vector<int64_t> up_off;       // per node offset (ints) into up_links, -1 if level 0 only
   std::vector<int32_t> up_links;     // concatenated upper-level lists, verbatim
   std::vector<int32_t> level;        // per node top level
+  // l2sqr_sift indices (regular graph file + objects file): no level0 block; the lists, vectors,
+  // norms and object ids are kept here, and M / the saved maxlevel for writing the file back
+  bool sift = false;
+  uint64_t M = 0;
+  int32_t saved_maxlevel = 0;
+  uint32_t cap0 = 0, capu = 0;       // longest level-0 / upper-level list
+  std::vector<int32_t> sift_l0;      // n x (cap0 + 1): count, then ids
+  std::vector<uint8_t> sift_vecs;    // n x 128
+  std::vector<int32_t> sift_norms;   // n, as stored with each object
+  std::vector<int32_t> sift_ids, sift_labels;
 
   const float* vec(int64_t i) const {
     return reinterpret_cast<const float*>(level0.data() + i * mem_per_obj + off_data + 16);
@@ -58,6 +75,10 @@ struct HostIndex {
 int read_index_file(const char* path, HostIndex& ix, std::string& err);
 int validate_index(const HostIndex& ix, std::string& err);
 int write_index_file(const char* path, const HostIndex& ix, std::string& err);
+// l2sqr_sift: the regular graph file (hnsw.cc:810-842 / 943-991) and the objects file
+// (python_bindings/nmslib.cc:98-125, space.cc WriteObjectVectorBinData). Validated on read.
+int read_sift_index(const char* graph_path, const char* data_path, HostIndex& ix, std::string& err);
+int write_sift_index(const char* graph_path, const char* data_path, const HostIndex& ix, std::string& err);
 
 // Device-resident index. Vectors are stored with a row pitch of round_up(dim, 32) floats and,
 // inside each 32-float chunk of the first (dim & ~15) elements, permuted so that lane j of an
@@ -66,6 +87,9 @@ int write_index_file(const char* path, const HostIndex& ix, std::string& err);
 // natural position. A final 16-float half chunk is permuted the same way into float2 pairs.
 struct DevIndex {
   const float* vecs = nullptr;      // [n][pitch]
+  const uint8_t* vecs_u8 = nullptr; // l2sqr_sift: [n][128]
+  const int32_t* norms = nullptr;   // l2sqr_sift: stored norms, or null when every stored norm is
+                                    // the sum of squares of its values (recomputed from the row)
   const int32_t* l0 = nullptr;      // [n][l0_pitch]: cnt, neighbour ids (internal)
   const int64_t* up_off = nullptr;  // [n]
   const int32_t* up_links = nullptr;
@@ -74,6 +98,7 @@ struct DevIndex {
   int dim = 0, pitch = 0, l0_pitch = 0;
   int n16 = 0, n4 = 0;
   int maxM = 0, maxM0 = 0, maxlevel = 0, enterpoint = 0, dist_type = 0;
+  int row_bytes = 0;                // algorithmic bytes of one row: 4 dim, or 132 for l2sqr_sift
 };
 
 // Position of element e of a vector in the permuted device row.
@@ -88,6 +113,8 @@ NMSG_HD inline int permuted_pos(int e, int dim) {
 struct SearchArgs {
   DevIndex ix;
   const float* queries = nullptr;   // [nq][dim]
+  const uint8_t* queries_u8 = nullptr;  // l2sqr_sift: [nq][128]
+  int dists_int = 0;                // write distances as int32 (l2sqr_sift)
   int64_t nq = 0;
   int k_default = 10, ef_default = 20, algo = 0;
   const int32_t* k_per_q = nullptr;

@@ -415,6 +415,7 @@ int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int
   d.pitch = (dim + 31) & ~31;
   d.n16 = dim & ~15;
   d.n4 = dim & ~3;
+  d.row_bytes = 4 * dim;
   d.maxM = b.maxM;
   d.maxM0 = b.maxM0;
   d.l0_pitch = b.l0_stride;

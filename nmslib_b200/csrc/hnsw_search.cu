@@ -196,7 +196,53 @@ __device__ void compute_dists(const DevIndex& ix, const float* __restrict__ q, c
   const int nfull = ix.n16 >> 5;
   const bool half = (ix.n16 & 31) != 0;
   const int code = ix.dist_type;
-  if constexpr (R == kLpGather) {  // L1 / LInf indices run kernels of their own (gather code 3)
+  if constexpr (R == kSiftGather) {
+    // l2sqr_sift: eight 4-lane groups, one 128-byte row per group; lane j of a group takes bytes
+    // [32j, 32j + 32) of the row and of the query (shared memory: 128 values, then the query's
+    // norm). The reference's distance |q|^2 + |x|^2 - 2 q.x in int (distcomp_l2sqr_sift.cc:40-50)
+    // is exact whatever the order of the products and sums, so byte dot products (dp4a) and a
+    // butterfly over the group give the same integer; it is below 2^24, so the float key is exact.
+    const int g4 = lane >> 2, j4 = lane & 3;
+    const uint4* qv = reinterpret_cast<const uint4*>(q) + 2 * j4;
+    const uint4 qa = qv[0], qb = qv[1];
+    const int qn = reinterpret_cast<const int*>(q)[kSiftDim / 4];
+    for (int base = 0; base < n; base += 8) {
+      const int idx = base + g4;
+      const bool act = idx < n;
+      const int id = act ? ids[idx] : 0;
+      uint4 xa = make_uint4(0u, 0u, 0u, 0u), xb = xa;
+      if (act) {
+        const uint4* row = reinterpret_cast<const uint4*>(ix.vecs_u8 + (int64_t)id * kSiftDim) + 2 * j4;
+        xa = __ldg(row);
+        xb = __ldg(row + 1);
+      }
+      unsigned dot = __dp4a(xa.x, qa.x, 0u);
+      dot = __dp4a(xa.y, qa.y, dot);
+      dot = __dp4a(xa.z, qa.z, dot);
+      dot = __dp4a(xa.w, qa.w, dot);
+      dot = __dp4a(xb.x, qb.x, dot);
+      dot = __dp4a(xb.y, qb.y, dot);
+      dot = __dp4a(xb.z, qb.z, dot);
+      dot = __dp4a(xb.w, qb.w, dot);
+      unsigned xx = __dp4a(xa.x, xa.x, 0u);
+      xx = __dp4a(xa.y, xa.y, xx);
+      xx = __dp4a(xa.z, xa.z, xx);
+      xx = __dp4a(xa.w, xa.w, xx);
+      xx = __dp4a(xb.x, xb.x, xx);
+      xx = __dp4a(xb.y, xb.y, xx);
+      xx = __dp4a(xb.z, xb.z, xx);
+      xx = __dp4a(xb.w, xb.w, xx);
+      dot += __shfl_xor_sync(kFull, dot, 1);
+      xx += __shfl_xor_sync(kFull, xx, 1);
+      dot += __shfl_xor_sync(kFull, dot, 2);
+      xx += __shfl_xor_sync(kFull, xx, 2);
+      if (act && j4 == 0) {
+        const int xn = ix.norms ? __ldg(ix.norms + id) : (int)xx;
+        out[idx] = __int2float_rn(qn + xn - 2 * (int)dot);
+      }
+    }
+    __syncwarp();
+  } else if constexpr (R == kLpGather) {  // L1 / LInf indices run kernels of their own (gather code 3)
     for (int base = 0; base < n; base += 4) {
       const int idx = base + g;
       const bool act = idx < n;
@@ -787,6 +833,18 @@ __device__ void visit_one(WarpCtx& w, int id) {
 __device__ void load_query(const SearchArgs& a, const WarpCtx& w, int64_t qi) {
   const DevIndex& ix = a.ix;
   const int lane = lane_id();
+  if (ix.dist_type == kSiftL2) {
+    // 128 uint8 values, then their int sum of squares (the query object's norm,
+    // space_l2sqr_sift.cc:137-150): exact in any order
+    const uint32_t word = reinterpret_cast<const uint32_t*>(a.queries_u8 + qi * kSiftDim)[lane];
+    reinterpret_cast<uint32_t*>(w.q)[lane] = word;
+    int s = (int)__dp4a(word, word, 0u);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    if (lane == 0) reinterpret_cast<int*>(w.q)[kSiftDim / 4] = s;
+    __syncwarp();
+    return;
+  }
   const float* src = a.queries + qi * ix.dim;
   // zero padding first (the permuted chunks read whole float4 / float2 groups)
   for (int e = lane; e < ix.pitch; e += 32) w.q[e] = 0.0f;
@@ -882,10 +940,10 @@ __device__ void greedy_descent(const SearchArgs& a, WarpCtx& w, int& cur_out, fl
   int cur = ix.enterpoint;
   if (lane == 0) w.nb_id[0] = cur;
   __syncwarp();
-  compute_dists<(R == kLpGather ? kLpGather : 1)>(ix, w.q, w.nb_id, 1, w.nb_d);
+  compute_dists<(R == kLpGather || R == kSiftGather ? R : 1)>(ix, w.q, w.nb_id, 1, w.nb_d);
   float curdist = w.nb_d[0];
   w.st_dist += 1;
-  w.st_bytes += 4LL * ix.dim;
+  w.st_bytes += ix.row_bytes;
   __syncwarp();
   for (int lev = ix.maxlevel; lev > 0; --lev) {
     bool changed = true;
@@ -898,7 +956,7 @@ __device__ void greedy_descent(const SearchArgs& a, WarpCtx& w, int& cur_out, fl
       dists<R>(a, w, w.nb_id, cnt, w.nb_d);
       w.st_greedy += 1;
       w.st_dist += cnt;
-      w.st_bytes += 4LL * (1 + cnt) + 4LL * ix.dim * cnt;
+      w.st_bytes += 4LL * (1 + cnt) + (int64_t)ix.row_bytes * cnt;
       // sequential scan with strict improvement == earliest position of the minimum below curdist
       float best = curdist;
       int bpos = 0x7fffffff;
@@ -949,10 +1007,16 @@ __device__ void write_result_row(const SearchArgs& a, int64_t qi, const uint2* r
         for (int t = s; t < e; ++t) rank += (int)(res[t].y & kIdMask) < ni;
       }
       a.ids[qi * a.kmax + rank] = __ldg(ix.ext_id + ni);
-      a.dists[qi * a.kmax + rank] = ki;
+      if (a.dists_int)  // l2sqr_sift: the key is an exact integer
+        reinterpret_cast<int32_t*>(a.dists)[qi * a.kmax + rank] = __float2int_rn(ki);
+      else
+        a.dists[qi * a.kmax + rank] = ki;
     } else {
       a.ids[qi * a.kmax + i] = -1;
-      a.dists[qi * a.kmax + i] = __int_as_float(0x7f800000);
+      if (a.dists_int)
+        reinterpret_cast<int32_t*>(a.dists)[qi * a.kmax + i] = 0x7fffffff;
+      else
+        a.dists[qi * a.kmax + i] = __int_as_float(0x7f800000);
     }
   }
   if (lane == 0) a.counts[qi] = cnt;
@@ -991,7 +1055,7 @@ __device__ void search_v1merge(const SearchArgs& a, WarpCtx& w, int64_t qi, int 
     w.st_bytes += 4LL * (1 + cnt);
     dists<R>(a, w, w.nb_id, nnew, w.nb_d);
     w.st_dist += nnew;
-    w.st_bytes += 4LL * ix.dim * nnew;
+    w.st_bytes += (int64_t)ix.row_bytes * nnew;
     // keep d < topKey || size < ef, preserving list order
     int qty = 0;
     for (int base = 0; base < nnew; base += 32) {
@@ -1077,7 +1141,7 @@ __device__ bool search_old(const SearchArgs& a, WarpCtx& w, int64_t qi, int k, i
     w.st_bytes += 4LL * (1 + cnt);
     dists<R>(a, w, w.nb_id, nnew, w.nb_d);
     w.st_dist += nnew;
-    w.st_bytes += 4LL * ix.dim * nnew;
+    w.st_bytes += (int64_t)ix.row_bytes * nnew;
     if (lane == 0) {
       for (int t = 0; t < nnew; ++t) {
         const float d = w.nb_d[t];
@@ -1748,6 +1812,7 @@ Kern pick(bool plain, int gather) {
       case 1: return search_plain_kernel<1, OLD>;
       case 2: return search_plain_kernel<2, OLD>;
       case kLpGather: return search_plain_kernel<kLpGather, OLD>;
+      case kSiftGather: return search_plain_kernel<kSiftGather, OLD>;
       default: return search_plain_kernel<4, OLD>;
     }
   }
@@ -1756,6 +1821,7 @@ Kern pick(bool plain, int gather) {
     case 1: return search_batched_kernel<1, OLD>;
     case 2: return search_batched_kernel<2, OLD>;
     case kLpGather: return search_batched_kernel<kLpGather, OLD>;
+    case kSiftGather: return search_batched_kernel<kSiftGather, OLD>;
     default: return search_batched_kernel<4, OLD>;
   }
 }

@@ -98,6 +98,10 @@ extern "C" NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* h, const float* queri
     set_last_error("nq must be >= 0, k >= 1 and kmax >= k");
     return NMSG_ERR_BAD_ARG;
   }
+  if (h->host.sift) {
+    set_last_error("nmsg_knn_batch_noalloc takes float queries; l2sqr_sift indices are searched with nmsg_knn_batch_u8");
+    return NMSG_ERR_BAD_ARG;
+  }
   if (nq > 0 && (!queries || !ids || !dists || !counts)) {
     set_last_error("null buffer");
     return NMSG_ERR_BAD_ARG;

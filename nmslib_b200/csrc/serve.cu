@@ -229,6 +229,7 @@ NMSG_API int nmsg_server_create(nmsg_index* h, int64_t memory_budget_bytes, int3
   *out = nullptr;
   const DevIndex& d = h->dev;
   if (d.n == 0) return srv_fail(NMSG_ERR_BAD_ARG, "the index is empty");
+  if (h->host.sift) return srv_fail(NMSG_ERR_UNSUPPORTED, "serving l2sqr_sift indices is not supported");
   auto* s = new nmsg_server();
   s->h = h;
   s->max_batch = max_batch;

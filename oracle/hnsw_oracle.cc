@@ -730,9 +730,10 @@ void oracle_sift_info(void* h, int64_t* info) {
 }
 
 // Batch search over nq x 128 uint8 queries; algo as oracle_search. Outputs nq x kmax object ids
-// and int distances, -1 / INT32_MAX padding.
+// and int distances, -1 / INT32_MAX padding; stats (optional) as oracle_search's, with 132 bytes
+// (values and norm) per row.
 int oracle_sift_search(void* h, const uint8_t* queries, int64_t nq, int k, int ef, int algo, int kmax, int32_t* ids,
-                       int32_t* dists, int32_t* counts, int nthreads) {
+                       int32_t* dists, int32_t* counts, int64_t* stats, int nthreads) {
   auto* ix = static_cast<SiftIndex*>(h);
   if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
   std::atomic<int64_t> next(0);
@@ -756,6 +757,12 @@ int oracle_sift_search(void* h, const uint8_t* queries, int64_t nq, int k, int e
       for (int j = 0; j < kmax; ++j) {
         ids[qi * kmax + j] = j < cnt ? ix->obj_ids[res[j].second] : -1;
         dists[qi * kmax + j] = j < cnt ? (int32_t)res[j].first : INT32_MAX;
+      }
+      if (stats) {
+        stats[qi * 4 + 0] = st.n_dist;
+        stats[qi * 4 + 1] = st.n_expand;
+        stats[qi * 4 + 2] = st.n_greedy;
+        stats[qi * 4 + 3] = st.bytes;
       }
     }
   };

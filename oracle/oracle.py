@@ -64,7 +64,7 @@ def _load():
         lib.oracle_sift_free.argtypes = [P]
         lib.oracle_sift_info.argtypes = [P, P]
         lib.oracle_sift_search.restype = I32
-        lib.oracle_sift_search.argtypes = [P, P, I64, I32, I32, I32, I32, P, P, P, I32]
+        lib.oracle_sift_search.argtypes = [P, P, I64, I32, I32, I32, I32, P, P, P, P, I32]
         lib.oracle_last_error.restype = ctypes.c_char_p
         _lib = lib
     return _lib
@@ -169,8 +169,10 @@ class OracleSiftIndex:
             _load().oracle_sift_free(self._h)
             self._h = None
 
-    def search(self, queries, k, ef, algo=0, nthreads=0):
-        """(ids [nq,k], int32 dists [nq,k], counts [nq]); algo 0 hybrid, 1 old, 2 v1merge."""
+    def search(self, queries, k, ef, algo=0, nthreads=0, stats=False):
+        """(ids [nq,k], int32 dists [nq,k], counts [nq][, stats [nq,4]]); algo 0 hybrid, 1 old,
+        2 v1merge. stats: distance evaluations, level-0 expansions, upper-level list scans,
+        algorithmic bytes."""
         q = np.ascontiguousarray(queries, np.uint8)
         if q.ndim != 2 or q.shape[1] != 128:
             raise ValueError("l2sqr_sift queries are [nq, 128] uint8")
@@ -178,11 +180,12 @@ class OracleSiftIndex:
         ids = np.empty((nq, k), np.int32)
         dists = np.empty((nq, k), np.int32)
         counts = np.empty(nq, np.int32)
+        st = np.zeros((nq, 4), np.int64)
         rc = _load().oracle_sift_search(self._h, _ptr(q), nq, int(k), int(ef), int(algo), int(k), _ptr(ids),
-                                        _ptr(dists), _ptr(counts), int(nthreads))
+                                        _ptr(dists), _ptr(counts), _ptr(st), int(nthreads))
         if rc != 0:
             raise ValueError(_load().oracle_last_error().decode())
-        return ids, dists, counts
+        return (ids, dists, counts, st) if stats else (ids, dists, counts)
 
 
 def bruteforce_fp64(base, queries, k, space, ids=None, chunk=256):
