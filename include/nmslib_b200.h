@@ -181,6 +181,10 @@ typedef struct nmsg_launch_config {
                                 blocks, a block that finds no free slot in one bounded pass gives up:
                                 its query returns nothing and the call fails with NMSG_ERR_TIMEOUT
                                 (a way to exercise that bounded wait) */
+  int32_t queries_per_warp;  /* persistent kernel: queries one warp carries at once (1..4); their
+                                list reads, visited checks and row copies overlap. Used for
+                                V1Merge batches over float rows staged in shared memory with lists
+                                of up to 64 ids; other batches run one query per warp */
 } nmsg_launch_config;
 
 /* Set (cfg != NULL) or reset to automatic (cfg == NULL) the launch shape used by later

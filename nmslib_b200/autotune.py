@@ -1,11 +1,13 @@
 """Launch-shape autotuner for the HNSW search kernels.
 
-The search kernels run one query per warp; what varies is how many query warps share a block,
-how a round of vector rows is gathered (asynchronous copies of 4..16 rows into shared memory,
-or 1..2 rows per 8-lane group in registers) and whether the visited set starts in a shared-memory
-hash table. None of it changes results (the GPU parity tests run every shape); all of it changes
-speed with the vector width, the beam size (efSearch) and the graph. ``autotune`` times the
-candidate shapes on the caller's own queries and leaves the fastest one set on the index.
+What varies is how many queries one persistent warp carries at once (1..4: their list reads,
+visited checks and row copies overlap), how many warps share a block, how a round of vector rows
+is gathered (asynchronous copies of 4..16 rows into shared memory, or 1..2 rows per 8-lane group
+in registers) and whether the visited set starts in a shared-memory hash table. None of it changes
+results (the GPU parity tests run every shape); all of it changes speed with the vector width, the
+beam size (efSearch, which sets the shared memory each query needs) and the batch size.
+``autotune`` times the candidate shapes on the caller's own queries and leaves the fastest one set
+on the index.
 """
 from __future__ import annotations
 
@@ -15,11 +17,16 @@ import numpy as np
 
 from . import _capi
 
-# (warps_per_block, rows_per_group, visited_hash_log2, stage_rows)
+# (warps_per_block, rows_per_group, visited_hash_log2, stage_rows, queries_per_warp)
 DEFAULT_CANDIDATES = (
-    (4, 0, -1, 4), (4, 0, -1, 8), (4, 0, -1, 12), (4, 0, -1, 16), (2, 0, -1, 8),
-    (4, 1, -1, -1), (4, 2, -1, -1), (4, 0, 10, 8),
+    (4, 0, -1, 8, 1), (2, 0, -1, 8, 1), (4, 2, -1, -1, 1),
+    (4, 0, -1, 8, 2), (4, 0, -1, 16, 2), (2, 0, -1, 8, 2),
+    (4, 0, -1, 8, 3), (4, 0, -1, 8, 4), (4, 0, -1, 16, 4), (2, 0, -1, 16, 4),
 )
+
+
+def _config(shape):
+    return _capi.LaunchConfig(shape[0], shape[1], shape[3], shape[2], 0, shape[4] if len(shape) > 4 else 0)
 
 
 def autotune(index, queries, k=10, ef=None, candidates=DEFAULT_CANDIDATES, reps=5):
@@ -46,7 +53,7 @@ def autotune(index, queries, k=10, ef=None, candidates=DEFAULT_CANDIDATES, reps=
 
     table = []
     for shape in candidates:
-        cfg = _capi.LaunchConfig(shape[0], shape[1], shape[3], shape[2])
+        cfg = _config(shape)
         _capi.check(lib.nmsg_set_launch_config(h, ctypes.byref(cfg)))
         run()
         torch.cuda.synchronize()
@@ -58,6 +65,6 @@ def autotune(index, queries, k=10, ef=None, candidates=DEFAULT_CANDIDATES, reps=
         torch.cuda.synchronize()
         table.append((shape, start.elapsed_time(end) / reps))
     best = min(table, key=lambda t: t[1])[0]
-    cfg = _capi.LaunchConfig(best[0], best[1], best[3], best[2])
+    cfg = _config(best)
     _capi.check(lib.nmsg_set_launch_config(h, ctypes.byref(cfg)))
     return best, table

@@ -199,6 +199,23 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
     p.stage_rows = (p.stage_rows + 1) / 2;
     p.warp_smem = warp_smem_bytes(d, p.region, p.nbpad, p.hash_log2, p.stage_rows);
   }
+  // several queries per warp (search_multi_kernel): V1Merge over staged float rows, lists of up
+  // to 64 ids, no shared-memory visited table
+  p.ctx = 1;
+  const int want_ctx = cfg.queries_per_warp ? cfg.queries_per_warp : kDefaultQueriesPerWarp;
+  if (!plain && !with_old && p.gather == 0 && p.hash_log2 == 0 && want_ctx > 1 && p.stage_rows <= 32 &&
+      std::max(d.maxM, d.maxM0) <= 64) {
+    const int nbpad = std::max(32, ((std::max(d.maxM, d.maxM0) + 31) / 32) * 32);
+    for (int c = want_ctx; c > 1; --c) {
+      const int ws = multi_warp_smem_bytes(d, p.region, nbpad, p.stage_rows, c);
+      if (ws <= kMaxSmemPerBlock) {
+        p.ctx = c;
+        p.nbpad = nbpad;
+        p.warp_smem = ws;
+        break;
+      }
+    }
+  }
   p.wpb = plain ? 1 : (cfg.warps_per_block ? cfg.warps_per_block : kWarpsPerBlock);
   while (p.wpb > 1 && p.wpb * p.warp_smem > kMaxSmemPerBlock) p.wpb >>= 1;
   if (p.wpb * p.warp_smem > kMaxSmemPerBlock) {
@@ -206,7 +223,8 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
     return NMSG_ERR_CAPACITY;
   }
   p.blocks_per_sm = 0;
-  const int rc = search_occupancy(plain, p.gather, with_old, p.wpb, p.wpb * p.warp_smem, &p.blocks_per_sm);
+  const int rc = search_occupancy(plain, p.gather, with_old, p.wpb, p.wpb * p.warp_smem, &p.blocks_per_sm, p.ctx,
+                                  multi_list_chunks(d));
   if (rc != 0 || p.blocks_per_sm < 1) {
     *err = "no resident block fits this configuration";
     return NMSG_ERR_DEVICE;
@@ -370,10 +388,11 @@ int nmsg_last_device_status(const nmsg_index* h) { return h ? h->last_status : N
 
 int nmsg_set_launch_config(nmsg_index* h, const nmsg_launch_config* cfg) {
   if (!h) return fail(NMSG_ERR_BAD_ARG, "null index");
-  nmsg_launch_config c{0, 0, 0, 0, 0};
+  nmsg_launch_config c{0, 0, 0, 0, 0, 0};
   if (cfg) {
     c = *cfg;
     if (c.plain_slots < 0) return fail(NMSG_ERR_BAD_ARG, "plain_slots must be >= 0");
+    if (c.queries_per_warp < 0 || c.queries_per_warp > 4) return fail(NMSG_ERR_BAD_ARG, "queries_per_warp must be 0..4");
     const int w = c.warps_per_block, r = c.rows_per_group, hl = c.visited_hash_log2, sr = c.stage_rows;
     if (!(w == 0 || w == 1 || w == 2 || w == 4)) return fail(NMSG_ERR_BAD_ARG, "warps_per_block must be 0, 1, 2 or 4");
     if (!(r == 0 || r == 1 || r == 2 || r == 4)) return fail(NMSG_ERR_BAD_ARG, "rows_per_group must be 0, 1, 2 or 4");
@@ -467,7 +486,8 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
   const int blocks = plain ? 0 : bps * h->num_sms;
   const int slots = plain ? (h->cfg.plain_slots > 0 ? std::min(h->cfg.plain_slots, bps * h->num_sms)
                                                    : bps * h->num_sms)
-                          : blocks * wpb;
+                          : blocks * wpb * plan.ctx;
+  a.ctx_per_warp = plan.ctx;
   // scratch
   const int64_t vpitch = ((d.n + 15) / 16) * 16;
   if (slots > h->slots || (int64_t)h->visited.bytes < (int64_t)slots * vpitch) {

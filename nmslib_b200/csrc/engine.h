@@ -139,10 +139,15 @@ struct SearchArgs {
   int hash_log2 = 0;                // shared-memory visited table of 2^hash_log2 ids (0: none)
   int stage_rows = 0;               // rows per staged-gather round (gather mode 0)
   int warp_smem = 0;                // bytes of shared memory per warp
+  int ctx_per_warp = 1;             // queries a persistent warp carries at once (search_multi_kernel)
 };
 
 // Per-warp shared memory needed for the given caps.
 int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int hash_log2, int stage_rows);
+// The several-queries-per-warp kernel: list chunks of 32 it reads (1 or 2; it takes lists of up to
+// 64 ids) and its shared memory per warp (ctx contexts plus the staging rows).
+int multi_list_chunks(const DevIndex& ix);
+int multi_warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int stage_rows, int ctx);
 
 // Launch / occupancy of the search kernels (defined in hnsw_search.cu). `gather` selects how
 // vector rows are fetched: 0 = asynchronous copies into shared memory (stage_rows per round),
@@ -177,6 +182,6 @@ int level0_select_and_link(const DevIndex& ix, int space, int M, int efc, int64_
                            int32_t* pend, int32_t* pend_cnt, int32_t* touched, int32_t* n_touched, void* stream);
 
 int search_occupancy(bool plain, int gather, bool with_old, int warps_per_block, int smem_per_block,
-                     int* blocks_per_sm);
+                     int* blocks_per_sm, int ctx = 1, int nch = 1);
 
 }  // namespace nmsg

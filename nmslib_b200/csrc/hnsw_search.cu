@@ -830,24 +830,24 @@ __device__ void visit_one(WarpCtx& w, int id) {
   __syncwarp();
 }
 
-__device__ void load_query(const SearchArgs& a, const WarpCtx& w, int64_t qi) {
+__device__ void load_query(const SearchArgs& a, float* qdst, int64_t qi) {
   const DevIndex& ix = a.ix;
   const int lane = lane_id();
   if (ix.dist_type == kSiftL2) {
     // 128 uint8 values, then their int sum of squares (the query object's norm,
     // space_l2sqr_sift.cc:137-150): exact in any order
     const uint32_t word = reinterpret_cast<const uint32_t*>(a.queries_u8 + qi * kSiftDim)[lane];
-    reinterpret_cast<uint32_t*>(w.q)[lane] = word;
+    reinterpret_cast<uint32_t*>(qdst)[lane] = word;
     int s = (int)__dp4a(word, word, 0u);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
-    if (lane == 0) reinterpret_cast<int*>(w.q)[kSiftDim / 4] = s;
+    if (lane == 0) reinterpret_cast<int*>(qdst)[kSiftDim / 4] = s;
     __syncwarp();
     return;
   }
   const float* src = a.queries + qi * ix.dim;
   // zero padding first (the permuted chunks read whole float4 / float2 groups)
-  for (int e = lane; e < ix.pitch; e += 32) w.q[e] = 0.0f;
+  for (int e = lane; e < ix.pitch; e += 32) qdst[e] = 0.0f;
   __syncwarp();
   float s = 1.0f;
   bool scale = false;
@@ -870,7 +870,7 @@ __device__ void load_query(const SearchArgs& a, const WarpCtx& w, int64_t qi) {
   for (int e = lane; e < ix.dim; e += 32) {
     float v = src[e];
     if (scale) v = __fmul_rn(v, s);
-    w.q[permuted_pos(e, ix.dim)] = v;
+    qdst[permuted_pos(e, ix.dim)] = v;
   }
   __syncwarp();
 }
@@ -1217,7 +1217,7 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
 
   const int k = a.k_per_q ? a.k_per_q[qi] : a.k_default;
   const int ef = a.ef_per_q ? a.ef_per_q[qi] : a.ef_default;
-  load_query(a, w, qi);
+  load_query(a, w.q, qi);
   int cur;
   float curdist;
   greedy_descent<R>(a, w, cur, curdist);
@@ -1281,6 +1281,464 @@ __global__ void __launch_bounds__(32, 32) search_plain_kernel(SearchArgs a) {
   run_query<R, OLD>(a, smem, slot, qi);
   __threadfence();
   if (lane == 0) atomicExch(a.slot_locks + slot, 0);
+}
+
+// ------------------------------------------------------------------ several queries per warp
+// search_multi_kernel<C, NCH>: a persistent warp owns C query contexts (C visited slots) and moves
+// every active one by one step per loop iteration. A step is exactly one step of the
+// single-query code above: the entry point's distance, one greedy-descent list at one level, or
+// one SearchV1Merge expansion (pop, list, visited check, distances, filter, merge, advance). Each
+// context therefore takes the same steps in the same order as a warp that owned it alone, and
+// its results and per-query counts are the same bit for bit. What changes is the overlap: the
+// contexts' list reads, then their visited-byte reads, then all their new rows (one shared
+// staging area, rounds of stage_rows asynchronous copies) are issued together, so C dependent
+// chains are in flight per warp for about the registers of one, and a small batch fills the GPU
+// in one wave. V1Merge only, float rows through shared memory, lists of up to 32 * NCH ids.
+
+struct MultiCtx {  // lane-uniform state of one context (shared memory; lane 0 writes)
+  int64_t qi;
+  int mode;        // kIdle, kEntry, kGreedy, kBeam
+  int k, ef;
+  int level, cur;  // greedy descent
+  float curdist;
+  int curr, num;   // level-0 beam (SortArrBI state)
+  float top_key;   // the expansion's topKey and size (hnsw_distfunc_opt.cc:216-222)
+  int size_now;
+  int cnt, nnew;
+  int st_dist, st_expand, st_greedy, st_list_ints;
+  int epoch;
+  int steps;       // steps taken; bounded (see multi_step_bound)
+};
+static_assert(sizeof(MultiCtx) % 16 == 0, "context state keeps 16-byte alignment");
+enum { kIdle = 0, kEntry = 1, kGreedy = 2, kBeam = 3 };
+
+__host__ __device__ inline int multi_ctx_bytes(const DevIndex& ix, int region_items, int nbpad) {
+  return ((ix.pitch * 4 + region_items * 8 + nbpad * 16 + (int)sizeof(MultiCtx)) + 15) & ~15;
+}
+
+// No query takes more steps than this: every level-0 expansion pops a node that was inserted
+// once (at most n), and each level of the descent moves at most n times before it drops a level.
+// A context past it has met a broken invariant; it stops with NMSG_ERR_TIMEOUT instead of looping.
+__device__ __forceinline__ int64_t multi_step_bound(const DevIndex& ix) {
+  return ix.n + (int64_t)(ix.maxlevel + 1) * (ix.n + 1) + 4;
+}
+
+struct MultiView {  // one context's shared-memory pieces
+  float* q;
+  uint2* items;
+  int* nb_id;
+  float* nb_d;
+  float* sk;
+  int* sv;
+  MultiCtx* st;
+};
+
+__device__ __forceinline__ MultiView multi_view(const SearchArgs& a, char* base, int c) {
+  MultiView v;
+  char* p = base + (size_t)c * multi_ctx_bytes(a.ix, a.region_items, a.nbpad);
+  v.q = reinterpret_cast<float*>(p);
+  v.items = reinterpret_cast<uint2*>(v.q + a.ix.pitch);
+  v.nb_id = reinterpret_cast<int*>(v.items + a.region_items);
+  v.nb_d = reinterpret_cast<float*>(v.nb_id + a.nbpad);
+  v.sk = v.nb_d + a.nbpad;
+  v.sv = reinterpret_cast<int*>(v.sk + a.nbpad);
+  v.st = reinterpret_cast<MultiCtx*>(v.sv + a.nbpad);
+  return v;
+}
+
+// Distance from the query (shared memory, permuted) to one staged row, by the 8 lanes of a group
+// (every lane of the warp takes part: combine shuffles across the whole warp).
+__device__ __forceinline__ float staged_row_dist(const DevIndex& ix, const float* __restrict__ q,
+                                                 const float* __restrict__ row) {
+  const int j = lane_id() & 7;
+  const int nfull = ix.n16 >> 5;
+  const int code = ix.dist_type;
+  float acc = 0.0f;
+#pragma unroll 4
+  for (int c = 0; c < nfull; ++c) {
+    const float4 qv = reinterpret_cast<const float4*>(q + c * 32)[j];
+    const float4 x = reinterpret_cast<const float4*>(row + c * 32)[j];
+    acc = fma_term(code, qv.x, x.x, acc);
+    acc = fma_term(code, qv.y, x.y, acc);
+    acc = fma_term(code, qv.z, x.z, acc);
+    acc = fma_term(code, qv.w, x.w, acc);
+  }
+  if (ix.n16 & 31) {
+    const float2 qv = reinterpret_cast<const float2*>(q + nfull * 32)[j];
+    const float2 x = reinterpret_cast<const float2*>(row + nfull * 32)[j];
+    acc = fma_term(code, qv.x, x.x, acc);
+    acc = fma_term(code, qv.y, x.y, acc);
+  }
+  return combine(ix, acc, row, q);
+}
+
+// Starts query `item` of the work list in a context: parameters, the slot's next epoch (the
+// visited bytes are cleared when the byte wraps, hnsw.h:582-589) and the query vector.
+__device__ void multi_start(const SearchArgs& a, const MultiView& v, int slot, int item) {
+  const int lane = lane_id();
+  const int64_t qi = a.order ? a.order[item] : item;
+  int ep = 0;
+  if (lane == 0) ep = a.epochs[slot] + 1;
+  ep = __shfl_sync(kFull, ep, 0);
+  if (ep == 256) {
+    uint4* p = reinterpret_cast<uint4*>(a.visited + (int64_t)slot * a.visited_pitch);
+    const int64_t n16 = a.visited_pitch / 16;
+    for (int64_t t = lane; t < n16; t += 32) p[t] = make_uint4(0, 0, 0, 0);
+    ep = 1;
+  }
+  load_query(a, v.q, qi);
+  if (lane == 0) {
+    a.epochs[slot] = (uint8_t)ep;
+    MultiCtx& st = *v.st;
+    st.qi = qi;
+    st.mode = kEntry;
+    st.k = a.k_per_q ? a.k_per_q[qi] : a.k_default;
+    st.ef = a.ef_per_q ? a.ef_per_q[qi] : a.ef_default;
+    st.epoch = ep;
+    st.steps = 0;
+    st.st_dist = st.st_expand = st.st_greedy = st.st_list_ints = 0;
+  }
+  __syncwarp();
+}
+
+// The context reached level 0: the beam starts from the descent's result (hnsw_distfunc_opt.cc:
+// 200-214); a beam that has nothing to expand (efSearch 0) finishes at once.
+__device__ void multi_beam_init(const SearchArgs& a, const MultiView& v, int slot) {
+  MultiCtx& st = *v.st;
+  if (lane_id() == 0) {
+    v.items[0] = make_item(st.curdist, st.cur, false);
+    a.visited[(int64_t)slot * a.visited_pitch + st.cur] = (uint8_t)st.epoch;
+    st.num = 1;
+    st.curr = 0;
+    st.mode = kBeam;
+  }
+  __syncwarp();
+}
+
+__device__ void multi_finish(const SearchArgs& a, const MultiView& v, bool ok) {
+  MultiCtx& st = *v.st;
+  const int64_t qi = st.qi;
+  write_result_row(a, qi, v.items, ok ? min(st.k, st.num) : 0, false);
+  if (a.stats && lane_id() == 0) {
+    a.stats[qi * 4 + 0] = st.st_dist;
+    a.stats[qi * 4 + 1] = st.st_expand;
+    a.stats[qi * 4 + 2] = st.st_greedy;
+    a.stats[qi * 4 + 3] = (int64_t)a.ix.row_bytes * st.st_dist + 4LL * st.st_list_ints;
+  }
+  __syncwarp();
+  if (lane_id() == 0) {
+    if (!ok) set_status(a.status, NMSG_ERR_TIMEOUT);
+    st.mode = kIdle;
+  }
+  __syncwarp();
+}
+
+template <int C, int NCH>
+__global__ void __launch_bounds__(128, 8) search_multi_kernel(SearchArgs a) {
+  extern __shared__ __align__(16) char smem[];
+  const DevIndex& ix = a.ix;
+  const int warp = threadIdx.x >> 5, lane = lane_id();
+  const int g = lane >> 3;
+  char* wbase = smem + warp * a.warp_smem;
+  const int wslot = blockIdx.x * (blockDim.x >> 5) + warp;
+  if ((wslot + 1) * C > a.num_slots) return;
+  float* stage = reinterpret_cast<float*>(wbase + (size_t)C * multi_ctx_bytes(ix, a.region_items, a.nbpad));
+  // a context's pieces are recomputed where they are used (a few integer operations) rather than
+  // kept in registers for the whole loop
+  auto V = [&](int c) { return multi_view(a, wbase, c); };
+#pragma unroll
+  for (int c = 0; c < C; ++c)
+    if (lane == 0) V(c).st->mode = kIdle;
+  __syncwarp();
+  bool drained = false;
+  const int nf4 = (ix.dim + 3) >> 2;  // 16-byte pieces of a row
+  const int64_t step_bound = multi_step_bound(ix);
+  while (true) {
+    // ---- refill idle contexts from the work counter
+    unsigned active = 0;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      if (V(c).st->mode == kIdle && !drained) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.work_counter, 1);
+        item = __shfl_sync(kFull, item, 0);
+        if (item < a.nq)
+          multi_start(a, V(c), wslot * C + c, item);
+        else
+          drained = true;
+      }
+      if (V(c).st->mode != kIdle) active |= 1u << c;
+    }
+    if (!active) break;
+
+    // ---- lists: issue every context's list read before using any of them
+    int lv[C][NCH], lcnt[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const MultiCtx& st = *V(c).st;
+      const int mode = st.mode;
+      const int32_t* lst = nullptr;
+      int maxcnt = 0;
+      if (mode == kGreedy) {
+        lst = ix.up_links + __ldg(ix.up_off + st.cur) + (int64_t)(ix.maxM + 1) * (st.level - 1);
+        maxcnt = ix.maxM;
+      } else if (mode == kBeam) {
+        const uint2 e = V(c).items[st.curr];
+        const int node = (int)(e.y & kIdMask);
+        lst = ix.l0 + (int64_t)node * ix.l0_pitch;
+        maxcnt = ix.maxM0;
+      }
+#pragma unroll
+      for (int h = 0; h < NCH; ++h) {
+        const int t = 32 * h + lane;
+        lv[c][h] = (lst && t < maxcnt) ? __ldg(lst + 1 + t) : -1;
+      }
+      lcnt[c] = lst ? __ldg(lst) : 0;
+    }
+    // beam contexts: mark the popped item used, note topKey and the size (hnsw_distfunc_opt.cc:
+    // 212-222); the next candidate's list is pulled into L2 (it is usually expanded next)
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      MultiCtx& st = *V(c).st;
+      if (st.mode == kBeam) {
+        const int curr = st.curr;
+        const int num = st.num;
+        if (lane == 0) {
+          V(c).items[curr].y |= kUsedBit;
+          st.curr = curr + 1;
+          st.top_key = key_of(V(c).items[num - 1]);
+          st.size_now = num;
+        }
+        if (lane < 2 && curr + 1 < num) {
+          const int nxt = (int)(V(c).items[curr + 1].y & kIdMask);
+          const int32_t* p = ix.l0 + (int64_t)nxt * ix.l0_pitch + 32 * lane;
+          if (32 * lane < ix.l0_pitch) prefetch_l2(p);
+        }
+      }
+    }
+    __syncwarp();
+    // ---- new neighbours: greedy lists are taken whole; beam lists go through the visited set,
+    // 32 entries at a time in list order (duplicates inside a list count once, as the reference's
+    // sequential check does), every context's visited bytes read before any is marked
+    int nnew[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      nnew[c] = 0;
+      const int mode = V(c).st->mode;
+      if (mode == kEntry) {
+        if (lane == 0) V(c).nb_id[0] = ix.enterpoint;
+        nnew[c] = 1;
+      } else if (mode == kGreedy) {
+#pragma unroll
+        for (int h = 0; h < NCH; ++h)
+          if (32 * h + lane < lcnt[c]) V(c).nb_id[32 * h + lane] = lv[c][h];
+        nnew[c] = lcnt[c];
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < NCH; ++h) {
+      uint8_t vb[C];
+      bool cand[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const MultiCtx& st = *V(c).st;
+        cand[c] = false;
+        vb[c] = 0;
+        if (st.mode == kBeam && 32 * h < lcnt[c]) {
+          const int t = 32 * h + lane;
+          const int id = t < lcnt[c] ? lv[c][h] : -1;
+          const unsigned same = __match_any_sync(kFull, id);
+          cand[c] = t < lcnt[c] && (__ffs(same) - 1) == lane;
+          if (cand[c]) vb[c] = a.visited[(int64_t)(wslot * C + c) * a.visited_pitch + id];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const MultiCtx& st = *V(c).st;
+        if (st.mode == kBeam && 32 * h < lcnt[c]) {
+          const int id = lv[c][h];
+          const bool isnew = cand[c] && vb[c] != (uint8_t)st.epoch;
+          if (isnew) a.visited[(int64_t)(wslot * C + c) * a.visited_pitch + id] = (uint8_t)st.epoch;
+          const unsigned m = __ballot_sync(kFull, isnew);
+          if (isnew) V(c).nb_id[nnew[c] + __popc(m & lanemask_lt())] = id;
+          nnew[c] += __popc(m);
+        }
+      }
+      __syncwarp();  // this chunk's marks are seen by the next chunk's reads (an id listed twice)
+    }
+    // ---- distances: every context's new rows through the staging area
+    int off[C + 1];
+    off[0] = 0;
+#pragma unroll
+    for (int c = 0; c < C; ++c) off[c + 1] = off[c] + nnew[c];
+    const int total = off[C];
+    for (int base = 0; base < total; base += a.stage_rows) {
+      const int cnt = min(a.stage_rows, total - base);
+      // lane r < cnt finds row r's vector, then the warp copies the rows one after another
+      const float* src_mine = ix.vecs;
+      if (lane < cnt) {
+        const int gr = base + lane;
+        int id = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+          if (gr >= off[c] && gr < off[c + 1]) id = V(c).nb_id[gr - off[c]];
+        src_mine = ix.vecs + (int64_t)id * ix.pitch;
+      }
+      for (int r = 0; r < cnt; ++r) {
+        const float* src = reinterpret_cast<const float*>(
+            __shfl_sync(kFull, reinterpret_cast<unsigned long long>(src_mine), r));
+        float* dst = stage + r * ix.pitch;
+        for (int f = lane; f < nf4; f += 32) cp_async16(dst + 4 * f, src + 4 * f);
+      }
+      cp_async_wait_all();
+      __syncwarp();
+      for (int r0 = 0; r0 < cnt; r0 += 4) {
+        const int r = r0 + g;
+        const bool act = r < cnt;
+        const int gr = base + (act ? r : 0);
+        int cc = 0;
+#pragma unroll
+        for (int c = 1; c < C; ++c)
+          if (gr >= off[c]) cc = c;
+        const float* q = V(0).q;
+        float* out = V(0).nb_d;
+#pragma unroll
+        for (int c = 1; c < C; ++c)
+          if (cc == c) {
+            q = V(c).q;
+            out = V(c).nb_d;
+          }
+        const float d = staged_row_dist(ix, q, stage + (act ? r : 0) * ix.pitch);
+        if (act && (lane & 7) == 0) out[gr - off[cc]] = d;
+      }
+      __syncwarp();
+    }
+    // ---- per context: what the step's distances mean
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      MultiCtx& st = *V(c).st;
+      const int mode = st.mode;
+      if (mode == kEntry) {
+        const float d0 = V(c).nb_d[0];
+        __syncwarp();
+        if (lane == 0) {
+          st.cur = ix.enterpoint;
+          st.curdist = d0;
+          st.st_dist += 1;
+          st.level = ix.maxlevel;
+          st.mode = kGreedy;
+        }
+        __syncwarp();
+        if (ix.maxlevel == 0) multi_beam_init(a, V(c), wslot * C + c);
+      } else if (mode == kGreedy) {
+        // hnsw_distfunc_opt.cc:168-198: the earliest strictly smaller distance of the list wins
+        const int cnt = lcnt[c];
+        const float curdist = st.curdist;
+        float best = curdist;
+        int bpos = 0x7fffffff;
+        for (int t = lane; t < cnt; t += 32) {
+          const float d = V(c).nb_d[t];
+          if (d < best || (d == best && d < curdist && t < bpos)) {
+            best = d;
+            bpos = t;
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const float ob = __shfl_xor_sync(kFull, best, o);
+          const int op = __shfl_xor_sync(kFull, bpos, o);
+          if (ob < best || (ob == best && op < bpos)) {
+            best = ob;
+            bpos = op;
+          }
+        }
+        const bool moved = bpos != 0x7fffffff && best < curdist;
+        const int next = moved ? V(c).nb_id[bpos] : 0;
+        __syncwarp();
+        if (lane == 0) {
+          st.st_greedy += 1;
+          st.st_dist += cnt;
+          st.st_list_ints += 1 + cnt;
+          if (moved) {
+            st.cur = next;
+            st.curdist = best;
+          } else {
+            st.level -= 1;
+          }
+        }
+        __syncwarp();
+        if (!moved && st.level == 0) multi_beam_init(a, V(c), wslot * C + c);
+      } else if (mode == kBeam) {
+        const float top_key = st.top_key;
+        const int size_now = st.size_now, ef = st.ef, k = st.k;
+        const int n_new = nnew[c];
+        // keep d < topKey || size < ef, preserving list order (hnsw_distfunc_opt.cc:237-247)
+        int qty = 0;
+        for (int b0 = 0; b0 < n_new; b0 += 32) {
+          const int t = b0 + lane;
+          bool keep = false;
+          float d = 0.0f;
+          int id = 0;
+          if (t < n_new) {
+            d = V(c).nb_d[t];
+            id = V(c).nb_id[t];
+            keep = (d < top_key) || (size_now < ef);
+          }
+          const unsigned m = __ballot_sync(kFull, keep);
+          if (keep) {
+            const int p = qty + __popc(m & lanemask_lt());
+            V(c).sk[p] = d;
+            V(c).sv[p] = id;
+          }
+          qty += __popc(m);
+        }
+        __syncwarp();
+        int num = st.num, curr = st.curr;
+        const int cap = max(ef, k);
+        if (qty) {
+          int p0;
+          if (merge_unsorted_batch(V(c).items, num, cap, V(c).sk, V(c).sv, qty, V(c).nb_d, V(c).nb_id, &p0)) {
+            if (p0 < curr) curr = p0;
+          } else {
+            sort_like_std(V(c).sk, V(c).sv, qty, V(c).nb_d, V(c).nb_id);
+            for (int i = 0; i < qty; ++i) {
+              const int ins = sorted_insert(V(c).items, num, cap, V(c).sk[i], V(c).sv[i]);
+              if (ins < curr) curr = ins;
+            }
+          }
+        }
+        // advance to the first unused item
+        while (curr < num) {
+          const int t = curr + lane;
+          const bool unused = t < num && !(V(c).items[t].y & kUsedBit);
+          const unsigned m = __ballot_sync(kFull, unused);
+          if (m) {
+            curr += __ffs(m) - 1;
+            break;
+          }
+          curr += 32;
+          if (curr > num) curr = num;
+        }
+        __syncwarp();
+        if (lane == 0) {
+          st.st_expand += 1;
+          st.st_dist += n_new;
+          st.st_list_ints += 1 + lcnt[c];
+          st.num = num;
+          st.curr = curr;
+        }
+        __syncwarp();
+      }
+      if (mode != kIdle) {
+        if (lane == 0) st.steps += 1;
+        __syncwarp();
+        if (st.mode == kBeam && !(st.curr < min(st.num, st.ef)))
+          multi_finish(a, V(c), true);
+        else if (st.mode != kIdle && st.steps > step_bound)
+          multi_finish(a, V(c), false);
+      }
+    }
+  }
 }
 
 // ------------------------------------------------------------------ exact scan on CUDA cores
@@ -1795,6 +2253,12 @@ int exact_scan_knn(const DevIndex& ix, const float* queries, int64_t nq, int k, 
   return (int)cudaGetLastError();
 }
 
+int multi_list_chunks(const DevIndex& ix) { return std::max(ix.maxM, ix.maxM0) <= 32 ? 1 : 2; }
+
+int multi_warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int stage_rows, int ctx) {
+  return ctx * multi_ctx_bytes(ix, region_items, nbpad) + stage_rows * ix.pitch * 4;
+}
+
 int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int hash_log2, int stage_rows) {
   int bytes = ix.pitch * 4 + region_items * 8 + nbpad * 16 + (hash_log2 > 0 ? (4 << hash_log2) : 0) +
               stage_rows * ix.pitch * 4;
@@ -1826,7 +2290,12 @@ Kern pick(bool plain, int gather) {
   }
 }
 
-Kern kernel_for(bool plain, int gather, bool with_old) {
+Kern kernel_for(bool plain, int gather, bool with_old, int ctx = 1, int nch = 1) {
+  if (ctx > 1 && !plain && !with_old && gather == 0) {
+    if (ctx == 2) return nch == 1 ? search_multi_kernel<2, 1> : search_multi_kernel<2, 2>;
+    if (ctx == 3) return nch == 1 ? search_multi_kernel<3, 1> : search_multi_kernel<3, 2>;
+    return nch == 1 ? search_multi_kernel<4, 1> : search_multi_kernel<4, 2>;
+  }
   return with_old ? pick<true>(plain, gather) : pick<false>(plain, gather);
 }
 }  // namespace
@@ -1847,7 +2316,7 @@ int allow_max_smem(const void* kern) {
 
 int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, int blocks, int warps_per_block,
                   void* stream) {
-  Kern kern = kernel_for(plain, gather, with_old);
+  Kern kern = kernel_for(plain, gather, with_old, a.ctx_per_warp, multi_list_chunks(a.ix));
   const int smem = a.warp_smem * (plain ? 1 : warps_per_block);
   const int rc = allow_max_smem((const void*)kern);
   if (rc != 0) return rc;
@@ -1859,8 +2328,8 @@ int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, in
 }
 
 int search_occupancy(bool plain, int gather, bool with_old, int warps_per_block, int smem_per_block,
-                     int* blocks_per_sm) {
-  Kern kern = kernel_for(plain, gather, with_old);
+                     int* blocks_per_sm, int ctx, int nch) {
+  Kern kern = kernel_for(plain, gather, with_old, ctx, nch);
   const int rc = allow_max_smem((const void*)kern);
   if (rc != 0) return rc;
   return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, 32 * (plain ? 1 : warps_per_block),

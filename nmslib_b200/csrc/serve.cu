@@ -115,6 +115,7 @@ struct nmsg_server {
     LaunchPlan plan;
     std::string err;
     nmsg_launch_config cfg = h->cfg;
+    cfg.queries_per_warp = 1;  // a lane's slots are sized for one query per warp
     int rc = plan_launch(d, cfg, std::max(r.ef, r.k), false, false, &plan, &err);
     if (rc != NMSG_OK) return rc;
     SearchArgs a;

@@ -241,3 +241,55 @@ def test_plain_kernel_slot_wait_gives_up_with_timeout():
         np.testing.assert_array_equal(ids, oi)
         np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
     assert _capi.load().nmsg_last_device_status(idx._h) == 0
+
+
+@pytest.mark.parametrize("qpw", [1, 2, 3, 4])
+@pytest.mark.parametrize("stage", [4, 8, 16])
+@pytest.mark.parametrize("name,si", [("c1_l2_d128", 0), ("c1_l2_d128", 6), ("sift_l2_ties", 1), ("cos_d100", 0),
+                                     ("negdot_d960", 1), ("dup_l2_d16", 2), ("tiny_l2_d20_sqids", 1),
+                                     ("one_l2_d3", 0)])
+def test_queries_per_warp_do_not_change_results(name, si, stage, qpw):
+    """Several queries per persistent warp (their list reads, visited checks and row copies
+    overlapping) take the single-query steps in the same order: ids, distances and per-query
+    counts are the oracle's, for every context count and staging depth."""
+    k, ef, algo = golden_manifest()[name]["settings"][si]
+    q = load_golden(name)["queries"]
+    idx = _gpu_index(name)
+    idx.setLaunchConfig(stage_rows=stage, queries_per_warp=qpw)
+    try:
+        idx.setQueryTimeParams({"efSearch": ef, "algoType": algo})
+        ids, d, cnt, st = idx.knnQueryBatchArrays(q, k, stats=True)
+        oi, od, oc, ost = _oracle(name).search(q, k=k, ef=ef, algo=ALGO_CODES[algo])
+        np.testing.assert_array_equal(cnt, oc)
+        np.testing.assert_array_equal(ids, oi)
+        np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
+        np.testing.assert_array_equal(st, ost)
+        # a batch smaller than the warps' contexts, and a single query
+        for sub in (q[:37], q[5:6]):
+            ids, d, cnt, st = idx.knnQueryBatchArrays(sub, k, stats=True)
+            oi, od, oc, ost = _oracle(name).search(sub, k=k, ef=ef, algo=ALGO_CODES[algo])
+            np.testing.assert_array_equal(ids, oi)
+            np.testing.assert_array_equal(st, ost)
+    finally:
+        idx.setLaunchConfig()
+
+
+def test_queries_per_warp_mixed_k_ef():
+    """Per-query k and efSearch (all V1Merge) with four queries per warp."""
+    name = "c1_l2_d128"
+    q = load_golden(name)["queries"]
+    rng = np.random.default_rng(7)
+    ks = rng.choice([1, 10, 100], len(q)).astype(np.int32)
+    efs = rng.integers(0, 600, len(q)).astype(np.int32)
+    idx = _gpu_index(name)
+    idx.setQueryTimeParams({"efSearch": 20, "algoType": "hybrid"})
+    idx.setLaunchConfig(queries_per_warp=4)
+    try:
+        ids, d, cnt, st = idx.knnQueryBatchArrays(q, ks, ef=efs, stats=True)
+    finally:
+        idx.setLaunchConfig()
+    oi, od, oc, ost = _oracle(name).search(q, k=int(ks.max()), ef=20, k_per_q=ks, ef_per_q=efs)
+    np.testing.assert_array_equal(cnt, oc)
+    np.testing.assert_array_equal(ids, oi)
+    np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
+    np.testing.assert_array_equal(st, ost)
