@@ -861,7 +861,7 @@ def main():
                 "sweep": sweep,
                 "launch": {"autotuned_shape": {"warps_per_block": best_shape[0], "rows_per_group": best_shape[1],
                                                "visited_hash_log2": best_shape[2], "stage_rows": best_shape[3],
-                                               "queries_per_warp": best_shape[4]},
+                                               "queries_per_warp": best_shape[4], "row_copy": best_shape[5]},
                            "cuda_graph": True},
                 "serving": serving,
                 "bruteforce": brute,

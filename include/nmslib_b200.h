@@ -185,6 +185,8 @@ typedef struct nmsg_launch_config {
                                 list reads, visited checks and row copies overlap. Used for
                                 V1Merge batches over float rows staged in shared memory with lists
                                 of up to 64 ids; other batches run one query per warp */
+  int32_t row_copy;          /* that kernel's row staging: 0 = automatic, 1 = 16-byte asynchronous
+                                copies spread over the lanes, 2 = one bulk copy (TMA unit) per row */
 } nmsg_launch_config;
 
 /* Set (cfg != NULL) or reset to automatic (cfg == NULL) the launch shape used by later

@@ -17,16 +17,17 @@ import numpy as np
 
 from . import _capi
 
-# (warps_per_block, rows_per_group, visited_hash_log2, stage_rows, queries_per_warp)
+# (warps_per_block, rows_per_group, visited_hash_log2, stage_rows, queries_per_warp, row_copy)
 DEFAULT_CANDIDATES = (
-    (4, 0, -1, 8, 1), (2, 0, -1, 8, 1), (4, 2, -1, -1, 1),
-    (4, 0, -1, 8, 2), (4, 0, -1, 16, 2), (2, 0, -1, 8, 2),
-    (4, 0, -1, 8, 3), (4, 0, -1, 8, 4), (4, 0, -1, 16, 4), (2, 0, -1, 16, 4),
+    (4, 0, -1, 8, 1, 0), (2, 0, -1, 8, 1, 0), (4, 2, -1, -1, 1, 0),
+    (4, 0, -1, 8, 2, 0), (4, 0, -1, 16, 2, 0), (2, 0, -1, 8, 2, 0), (4, 0, -1, 8, 2, 2),
+    (4, 0, -1, 8, 3, 0), (4, 0, -1, 8, 4, 0), (4, 0, -1, 16, 4, 0), (2, 0, -1, 16, 4, 0), (4, 0, -1, 16, 4, 2),
 )
 
 
 def _config(shape):
-    return _capi.LaunchConfig(shape[0], shape[1], shape[3], shape[2], 0, shape[4] if len(shape) > 4 else 0)
+    return _capi.LaunchConfig(shape[0], shape[1], shape[3], shape[2], 0, shape[4] if len(shape) > 4 else 0,
+                              shape[5] if len(shape) > 5 else 0)
 
 
 def autotune(index, queries, k=10, ef=None, candidates=DEFAULT_CANDIDATES, reps=5):

@@ -2,11 +2,13 @@
 
     python -m nmslib_b200.build          # or: from nmslib_b200.build import build; build()
 
-nvcc compiles every source under nmslib_b200/csrc for sm_100a only (no PTX for other targets)
-and links one shared library exporting the C ABI of include/nmslib_b200.h.
+nvcc compiles every source under nmslib_b200/csrc for sm_100a only (no PTX for other targets),
+each on its own core into nmslib_b200/_build/, and links one shared library exporting the C ABI
+of include/nmslib_b200.h.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import hashlib
 import os
@@ -23,8 +25,9 @@ NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-Xcompiler", "-fPIC,-O3,-fvisibility=hidden",
-    "-shared", "--expt-relaxed-constexpr",
+    "--expt-relaxed-constexpr",
 ]
+OBJ_DIR = os.path.join(HERE, "_build")
 
 
 def _nvcc() -> str:
@@ -39,11 +42,13 @@ def _sources():
 
 
 def _digest() -> str:
+    """Digest of every source, header and flag, by path relative to the repository, so a copy of
+    the tree elsewhere (with its built library) is recognised as up to date."""
     h = hashlib.sha256()
     for p in _sources() + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + [
             os.path.join(ROOT, "include", "nmslib_b200.h")]:
         with open(p, "rb") as f:
-            h.update(p.encode() + f.read())
+            h.update(os.path.relpath(p, ROOT).encode() + f.read())
     h.update(" ".join(NVCC_FLAGS).encode())
     return h.hexdigest()
 
@@ -54,8 +59,23 @@ def build(force: bool = False, verbose: bool = False) -> str:
         with open(STAMP) as f:
             if f.read().strip() == digest:
                 return LIB
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    nvcc = _nvcc()
+    inc = ["-I", os.path.join(ROOT, "include")]
+
+    def compile_one(src):
+        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        cmd = [nvcc, *NVCC_FLAGS, *inc, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        return obj
+
+    # every source compiles on its own core; then one link
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+        objs = list(pool.map(compile_one, _sources()))
     tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-o", tmp, *_sources(), "-lcudart"]
+    cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

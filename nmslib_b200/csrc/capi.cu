@@ -215,6 +215,21 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
         break;
       }
     }
+    if (p.ctx > 1)
+      p.bulk_rows = cfg.row_copy == 2 || (cfg.row_copy == 0 && d.dim * 4 >= kBulkRowMinBytes);
+  }
+  // the lean kernel: V1Merge with one query per warp over the index shapes it is compiled for,
+  // rows staged by bulk copies (row_copy 1 asks for the 16-byte copies of the general kernel)
+  p.lean = false;
+  if (!plain && !with_old && p.gather == 0 && p.hash_log2 == 0 && p.ctx == 1 && cfg.row_copy != 1 &&
+      lean_supported(d)) {
+    const int nbpad = std::max(32, ((std::max(d.maxM, d.maxM0) + 31) / 32) * 32);
+    const int ws = lean_smem_bytes(d, p.region, nbpad, p.stage_rows);
+    if (ws <= kMaxSmemPerBlock) {
+      p.lean = true;
+      p.nbpad = nbpad;
+      p.warp_smem = ws;
+    }
   }
   p.wpb = plain ? 1 : (cfg.warps_per_block ? cfg.warps_per_block : kWarpsPerBlock);
   while (p.wpb > 1 && p.wpb * p.warp_smem > kMaxSmemPerBlock) p.wpb >>= 1;
@@ -223,8 +238,9 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
     return NMSG_ERR_CAPACITY;
   }
   p.blocks_per_sm = 0;
-  const int rc = search_occupancy(plain, p.gather, with_old, p.wpb, p.wpb * p.warp_smem, &p.blocks_per_sm, p.ctx,
-                                  multi_list_chunks(d));
+  const int rc = p.lean ? lean_occupancy(d, p.wpb, p.wpb * p.warp_smem, &p.blocks_per_sm)
+                        : search_occupancy(plain, p.gather, with_old, p.wpb, p.wpb * p.warp_smem, &p.blocks_per_sm,
+                                           p.ctx, multi_list_chunks(d));
   if (rc != 0 || p.blocks_per_sm < 1) {
     *err = "no resident block fits this configuration";
     return NMSG_ERR_DEVICE;
@@ -388,11 +404,12 @@ int nmsg_last_device_status(const nmsg_index* h) { return h ? h->last_status : N
 
 int nmsg_set_launch_config(nmsg_index* h, const nmsg_launch_config* cfg) {
   if (!h) return fail(NMSG_ERR_BAD_ARG, "null index");
-  nmsg_launch_config c{0, 0, 0, 0, 0, 0};
+  nmsg_launch_config c{0, 0, 0, 0, 0, 0, 0};
   if (cfg) {
     c = *cfg;
     if (c.plain_slots < 0) return fail(NMSG_ERR_BAD_ARG, "plain_slots must be >= 0");
     if (c.queries_per_warp < 0 || c.queries_per_warp > 4) return fail(NMSG_ERR_BAD_ARG, "queries_per_warp must be 0..4");
+    if (c.row_copy < 0 || c.row_copy > 2) return fail(NMSG_ERR_BAD_ARG, "row_copy must be 0, 1 or 2");
     const int w = c.warps_per_block, r = c.rows_per_group, hl = c.visited_hash_log2, sr = c.stage_rows;
     if (!(w == 0 || w == 1 || w == 2 || w == 4)) return fail(NMSG_ERR_BAD_ARG, "warps_per_block must be 0, 1, 2 or 4");
     if (!(r == 0 || r == 1 || r == 2 || r == 4)) return fail(NMSG_ERR_BAD_ARG, "rows_per_group must be 0, 1, 2 or 4");
@@ -488,6 +505,8 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
                                                    : bps * h->num_sms)
                           : blocks * wpb * plan.ctx;
   a.ctx_per_warp = plan.ctx;
+  a.bulk_rows = plan.bulk_rows ? 1 : 0;
+  a.lean = plan.lean ? 1 : 0;
   // scratch
   const int64_t vpitch = ((d.n + 15) / 16) * 16;
   if (slots > h->slots || (int64_t)h->visited.bytes < (int64_t)slots * vpitch) {

@@ -140,6 +140,9 @@ struct SearchArgs {
   int stage_rows = 0;               // rows per staged-gather round (gather mode 0)
   int warp_smem = 0;                // bytes of shared memory per warp
   int ctx_per_warp = 1;             // queries a persistent warp carries at once (search_multi_kernel)
+  int bulk_rows = 0;                // search_multi_kernel: stage each row with one bulk copy (TMA
+                                    // unit, mbarrier completion) instead of 16-byte copies per lane
+  int lean = 0;                     // run search_lean_kernel (V1Merge, common index shapes)
 };
 
 // Per-warp shared memory needed for the given caps.
@@ -148,6 +151,22 @@ int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int hash_lo
 // 64 ids) and its shared memory per warp (ctx contexts plus the staging rows).
 int multi_list_chunks(const DevIndex& ix);
 int multi_warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int stage_rows, int ctx);
+// The lean one-query-per-warp kernel (V1Merge; l2 / cosine / negdot rows of 16, 48, 64, 96, 128 or
+// 256 floats; lists of up to 64 ids): whether it covers an index, its occupancy and its shared
+// memory per warp.
+bool lean_supported(const DevIndex& ix);
+// The lean kernel for an index of the matching distance (lean_l2.cu / lean_cos.cu /
+// lean_negdot.cu), or null when its row or list length has no instantiation.
+void* lean_kernel_l2(const DevIndex& ix);
+void* lean_kernel_cos(const DevIndex& ix);
+void* lean_kernel_negdot(const DevIndex& ix);
+NMSG_HD inline int lean_warp_smem_bytes(int dim, int region_items, int nbpad, int stage_rows) {
+  return region_items * 8 + nbpad * 16 + stage_rows * dim * 4 + 16;  // + the row mbarrier
+}
+int lean_occupancy(const DevIndex& ix, int warps_per_block, int smem_per_block, int* blocks_per_sm);
+int lean_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int stage_rows);
+// Bytes one bulk row copy moves: the row rounded up to 16 bytes (the padding is zeros).
+NMSG_HD inline int bulk_row_bytes(const DevIndex& ix) { return ((ix.dim * 4 + 15) / 16) * 16; }
 
 // Launch / occupancy of the search kernels (defined in hnsw_search.cu). `gather` selects how
 // vector rows are fetched: 0 = asynchronous copies into shared memory (stage_rows per round),

@@ -20,7 +20,9 @@ void set_last_error(const std::string& msg);
 
 constexpr int kWarpsPerBlock = 4;
 // Queries a persistent warp carries at once unless the launch configuration says otherwise.
-constexpr int kDefaultQueriesPerWarp = 2;
+constexpr int kDefaultQueriesPerWarp = 1;
+// Rows wider than this many bytes are staged with one bulk copy each unless configured otherwise.
+constexpr int kBulkRowMinBytes = 1024;
 constexpr int kMaxSmemPerBlock = 227 * 1024;
 
 // Launch shape of one search launch (see plan_launch).
@@ -35,6 +37,8 @@ struct LaunchPlan {
   int blocks_per_sm = 0;
   bool with_old = false;
   int ctx = 1;            // queries per persistent warp (> 1: search_multi_kernel)
+  bool bulk_rows = false; // search_multi_kernel stages rows with bulk copies
+  bool lean = false;      // search_lean_kernel
 };
 
 // Chooses gather mode, shared-memory sizes and warps per block for a launch whose largest query
@@ -99,7 +103,7 @@ struct nmsg_index {
   int64_t old_cap = 0;      // entries per slot in old_heap
   int64_t resident_bytes = 0;
   int last_status = NMSG_OK;
-  nmsg_launch_config cfg{0, 0, 0, 0, 0, 0};
+  nmsg_launch_config cfg{0, 0, 0, 0, 0, 0, 0};
   nmsg::BruteForceState* bf = nullptr;  // brute-force data, built on first use
   cudaGraphExec_t graph_exec = nullptr;  // last captured device-pointer search (NMSG_CUDA_GRAPH)
   cudaStream_t capture_stream = nullptr;

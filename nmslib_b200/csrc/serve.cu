@@ -139,6 +139,7 @@ struct nmsg_server {
     a.hash_log2 = plan.hash_log2;
     a.stage_rows = plan.stage_rows;
     a.warp_smem = plan.warp_smem;
+    a.lean = plan.lean ? 1 : 0;
     const int wpb = plan.wpb;
     int blocks = std::min((r.nq + wpb - 1) / wpb, lane_slots / wpb);
     if (blocks < 1) blocks = 1;

@@ -243,19 +243,21 @@ def test_plain_kernel_slot_wait_gives_up_with_timeout():
     assert _capi.load().nmsg_last_device_status(idx._h) == 0
 
 
+@pytest.mark.parametrize("row_copy", [1, 2], ids=["cp16", "bulk"])
 @pytest.mark.parametrize("qpw", [1, 2, 3, 4])
 @pytest.mark.parametrize("stage", [4, 8, 16])
 @pytest.mark.parametrize("name,si", [("c1_l2_d128", 0), ("c1_l2_d128", 6), ("sift_l2_ties", 1), ("cos_d100", 0),
                                      ("negdot_d960", 1), ("dup_l2_d16", 2), ("tiny_l2_d20_sqids", 1),
                                      ("one_l2_d3", 0)])
-def test_queries_per_warp_do_not_change_results(name, si, stage, qpw):
+def test_queries_per_warp_do_not_change_results(name, si, stage, qpw, row_copy):
     """Several queries per persistent warp (their list reads, visited checks and row copies
     overlapping) take the single-query steps in the same order: ids, distances and per-query
-    counts are the oracle's, for every context count and staging depth."""
+    counts are the oracle's, for every context count, staging depth and row-copy kind (16-byte
+    copies per lane, or one bulk copy per row)."""
     k, ef, algo = golden_manifest()[name]["settings"][si]
     q = load_golden(name)["queries"]
     idx = _gpu_index(name)
-    idx.setLaunchConfig(stage_rows=stage, queries_per_warp=qpw)
+    idx.setLaunchConfig(stage_rows=stage, queries_per_warp=qpw, row_copy=row_copy)
     try:
         idx.setQueryTimeParams({"efSearch": ef, "algoType": algo})
         ids, d, cnt, st = idx.knnQueryBatchArrays(q, k, stats=True)
