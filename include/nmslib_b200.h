@@ -254,6 +254,23 @@ NMSG_API int nmsg_server_run_trace(nmsg_server* server, const float* queries, co
                                    int64_t nreq, double* latency_s, double* wall_s);
 NMSG_API void nmsg_server_free(nmsg_server* server);
 
+/* ---- Query server: NMSLIB's Thrift QueryService (query_server/protocol.thrift;
+ * query_server/cpp_client_server/QueryService_server.cpp:150-640) on a TCP port, binary protocol
+ * over a buffered (unframed) stream, in front of a loaded index, so the reference's clients work
+ * unchanged. knnQuery / knnQueryBatch return ReplyEntry lists in ascending distance
+ * (QueryService_server.cpp:392-440); setQueryTimeParams("efSearch=64,algoType=v1merge") waits for
+ * the queries in flight; rangeQuery answers QueryException "Range search is not supported!"
+ * (hnsw.cc:712-715); getDistance computes the space's distance of two text objects on the GPU.
+ * Float indices are searched through the continuous-batching serving loop where it applies.
+ * port 0 picks a free port (nmsg_query_server_port tells which); at most max_connections clients
+ * are served at once. The server uses the index's query-time parameters; do not change them
+ * through other calls while it runs. */
+typedef struct nmsg_query_server nmsg_query_server;
+NMSG_API int nmsg_query_server_start(nmsg_index* index, int port, int max_connections, int debug,
+                                     nmsg_query_server** out);
+NMSG_API int nmsg_query_server_port(const nmsg_query_server* server);
+NMSG_API void nmsg_query_server_stop(nmsg_query_server* server);
+
 /* Device status of the last batch on this handle (NMSG_OK or a device-side error code). */
 NMSG_API int nmsg_last_device_status(const nmsg_index* index);
 

@@ -102,6 +102,12 @@ def load(path: str = LIB_PATH):
     lib.nmsg_build_index_device.restype = ctypes.c_int
     lib.nmsg_build_last_error.argtypes = []
     lib.nmsg_build_last_error.restype = ctypes.c_char_p
+    lib.nmsg_query_server_start.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
+    lib.nmsg_query_server_start.restype = ctypes.c_int
+    lib.nmsg_query_server_port.argtypes = [P]
+    lib.nmsg_query_server_port.restype = ctypes.c_int
+    lib.nmsg_query_server_stop.argtypes = [P]
+    lib.nmsg_query_server_stop.restype = None
     lib.nmsg_last_error.argtypes = []
     lib.nmsg_last_error.restype = ctypes.c_char_p
     _lib = lib
