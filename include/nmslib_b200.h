@@ -68,8 +68,11 @@ enum nmsg_flags {
   NMSG_DEVICE_PTRS = 1, /* queries and outputs are device pointers; no host copies, no sync */
   NMSG_PLAIN_KERNEL = 2, /* one query per CUDA block (the unbatched kernel) instead of the
                            persistent work-queue kernel */
-  NMSG_CUDA_GRAPH = 4    /* with NMSG_DEVICE_PTRS: launch through a CUDA graph captured on the
+  NMSG_CUDA_GRAPH = 4,   /* with NMSG_DEVICE_PTRS: launch through a CUDA graph captured on the
                            first call and replayed while every argument stays the same */
+  NMSG_EXACT_SCAN = 8    /* nmsg_bruteforce_knn: scan on CUDA cores with the search's own distance
+                           arithmetic (every distance bit-identical to the HNSW search's) instead
+                           of the tensor-core path */
 };
 
 typedef struct nmsg_index_info {
@@ -217,9 +220,11 @@ NMSG_API int nmsg_knn_batch_noalloc(nmsg_index* index, const float* queries, int
  * reaches; a second BF16 GEMM over the whole base collects the vectors at or above it and the
  * exact rerank orders them. The ids are the exact top-k (ties by id); distances follow the
  * index's space as the HNSW path reports them (squared L2, 1 - cos on normalised vectors, -dot).
- * k <= 32. That is the path for l2 / cosinesimil / negdotprod with dim <= 256; L1, LInf and wider
- * rows are scanned exactly on CUDA cores with the query path's own distance arithmetic (every
- * distance bit-identical to the HNSW search's; stats then {0, n, 0, chunks}). The full scan keeps
+ * k <= 32. That is the path for l2 / cosinesimil / negdotprod rows of up to 4096 floats (up to 256
+ * the query block stays in shared memory, wider rows stream its K-blocks beside the base's); L1,
+ * LInf, wider rows and calls with NMSG_EXACT_SCAN are scanned exactly on CUDA cores with the query
+ * path's own distance arithmetic (every distance bit-identical to the HNSW search's; stats then
+ * {0, n, 0, chunks}). The full scan keeps
  * up to 64 vectors per query and per half of a base
  * chunk; a query that finds more in some chunk is scanned again with a raised threshold (up to
  * three times), and if it still overflows the call returns NMSG_ERR_CAPACITY (many vectors tied

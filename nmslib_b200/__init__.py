@@ -263,11 +263,12 @@ class FloatIndex:
                                                 flags, None))
         return (ids, dists, counts, st) if stats else (ids, dists, counts)
 
-    def bruteForceBatchArrays(self, queries, k=10, stats=False):
+    def bruteForceBatchArrays(self, queries, k=10, stats=False, exact_scan=False):
         """Exact k-NN over every stored vector (seq_search semantics) on the tensor cores:
         (ids [nq, k] external, dists [nq, k], counts [nq][, stats [4]]). k <= 32. l2 / cosinesimil /
-        negdotprod rows of up to 256 floats use BF16 tensor cores with an exact rerank; L1, LInf
-        and wider rows an exact CUDA-core scan."""
+        negdotprod rows of up to 4096 floats use BF16 tensor cores with an exact rerank; L1, LInf,
+        wider rows and ``exact_scan=True`` an exact CUDA-core scan whose distances are the search's
+        own values bit for bit."""
         h = self._require()
         q = self._queries(queries)
         nq = q.shape[0]
@@ -278,7 +279,8 @@ class FloatIndex:
         ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
         dim = q.shape[1] if nq else (self._info.dim if self._info else 0)
         _capi.check(_capi.load().nmsg_bruteforce_knn(h, ptr(q), nq, dim, int(k), int(k), ptr(ids), ptr(dists),
-                                                     ptr(counts), ptr(st), 0, None))
+                                                     ptr(counts), ptr(st),
+                                                     _capi.FLAG_EXACT_SCAN if exact_scan else 0, None))
         return (ids, dists, counts, st) if stats else (ids, dists, counts)
 
     def knnQueryBatch(self, queries, k=10, num_threads=0):

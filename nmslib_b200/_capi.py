@@ -19,7 +19,7 @@ ERR_DEVICE, ERR_TIMEOUT, ERR_CORRUPT_GRAPH, ERR_CAPACITY = -5, -6, -7, -8
 
 SPACE_L2, SPACE_COSINE, SPACE_NEGDOT, SPACE_L1, SPACE_LINF, SPACE_L2SQR_SIFT = 0, 1, 2, 3, 4, 5
 ALGO_HYBRID, ALGO_OLD, ALGO_V1MERGE = 0, 1, 2
-FLAG_DEVICE_PTRS, FLAG_PLAIN_KERNEL, FLAG_CUDA_GRAPH = 1, 2, 4
+FLAG_DEVICE_PTRS, FLAG_PLAIN_KERNEL, FLAG_CUDA_GRAPH, FLAG_EXACT_SCAN = 1, 2, 4, 8
 
 
 class IndexInfo(ctypes.Structure):

@@ -45,7 +45,8 @@ constexpr int BM = 128;                 // queries per tile = TMEM lanes
 constexpr int BN = 256;                 // base rows per tile = accumulator columns
 constexpr int BK = 64;                  // bf16 elements per 128-byte swizzle row
 constexpr int CAND = 32;                // candidates kept per query per list (pass A)
-constexpr int KB_MAX = 4;               // padded dim <= 256
+constexpr int KB_MAX = 4;               // padded dim <= 256 with the query block resident
+constexpr int KB_STREAM_MAX = 64;       // padded dim <= 4096 with query K-blocks streamed per stage
 constexpr int Q_BLOCK_BYTES = BM * BK * 2;   // 16 KB
 constexpr int X_STAGE_BYTES = BN * BK * 2;   // 32 KB
 constexpr int EPI_WARPS = 8;            // two warps per TMEM lane quarter, one per column half
@@ -56,7 +57,9 @@ constexpr int kCollectLen = 64;         // entries of a full-scan list (query, c
 
 struct GemmArgs {
   int kb;             // padded dim / 64
-  int stages;         // base-tile pipeline depth (3 when kb <= 2, else 2)
+  int stages;         // base-tile pipeline depth (3 when kb <= 2, else 2; 3 when streaming)
+  int stream_q;       // 1: rows wider than 256: each stage carries the query block's K-block with the
+                      // base K-block (the whole query block does not fit in shared memory)
   int n;              // base rows
   int nq;             // queries
   int n_tiles;        // tiles visited: tile j of the scan is base tile j * tile_step
@@ -79,13 +82,16 @@ struct GemmArgs {
   int32_t* status;
 };
 
-// Shared memory: Q blocks | base stages | candidate lists | barriers (1024-aligned base).
+// Shared memory: Q blocks | base stages | candidate lists | barriers (1024-aligned base). When the
+// query is streamed there is no resident Q region and each stage is a base K-block followed by
+// the query block's K-block.
 struct SmemLayout {
-  int q_off, x_off, key_off, id_off, nrm_off, bar_off, total;
-  __host__ __device__ SmemLayout(int kb, int stages) {
+  int q_off, x_off, stage_bytes, key_off, id_off, nrm_off, bar_off, total;
+  __host__ __device__ SmemLayout(int kb, int stages, int stream_q) {
     q_off = 0;
-    x_off = q_off + kb * Q_BLOCK_BYTES;
-    key_off = x_off + stages * X_STAGE_BYTES;
+    x_off = q_off + (stream_q ? 0 : kb * Q_BLOCK_BYTES);
+    stage_bytes = X_STAGE_BYTES + (stream_q ? Q_BLOCK_BYTES : 0);
+    key_off = x_off + stages * stage_bytes;
     id_off = key_off + HALVES * BM * LIST_STRIDE * 4;
     nrm_off = id_off + HALVES * BM * LIST_STRIDE * 4;  // per epilogue warp: its 128 columns' |x|^2
     bar_off = (nrm_off + EPI_WARPS * (BN / HALVES) * 4 + 7) & ~7;
@@ -166,7 +172,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     bf16_scan_kernel(const __grid_constant__ CUtensorMap tmq, const __grid_constant__ CUtensorMap tmx, GemmArgs a) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L(a.kb, a.stages);
+  const SmemLayout L(a.kb, a.stages, a.stream_q);
+  const int sbytes = L.stage_bytes;
   uint8_t* sq = base + L.q_off;
   uint8_t* sx = base + L.x_off;
   float* skey = reinterpret_cast<float*>(base + L.key_off);
@@ -223,7 +230,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int item = next_active_item<MODE>(a, blockIdx.x, n_items); item < n_items && ok;
            item = next_active_item<MODE>(a, item + gridDim.x, n_items)) {
         const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
-        if (qb != prev_qb) {
+        if (qb != prev_qb && !a.stream_q) {
           if (prev_qb >= 0) {
             ok = mbar_wait(q_empty, qphase);
             qphase ^= 1;
@@ -240,8 +247,9 @@ __global__ void __launch_bounds__(kThreads, 1)
           for (int kb = 0; kb < a.kb && ok; ++kb) {
             ok = mbar_wait(&x_empty[stage], xphase ^ 1);
             if (!ok) break;
-            mbar_arrive_expect_tx(&x_full[stage], X_STAGE_BYTES);
-            tma_load_2d(sx + stage * X_STAGE_BYTES, &tmx, &x_full[stage], kb * BK, t * BN);
+            mbar_arrive_expect_tx(&x_full[stage], (uint32_t)sbytes);
+            tma_load_2d(sx + stage * sbytes, &tmx, &x_full[stage], kb * BK, t * BN);
+            if (a.stream_q) tma_load_2d(sx + stage * sbytes + X_STAGE_BYTES, &tmq, &x_full[stage], kb * BK, qb * BM);
             ++x_armed;
             if (++stage == stages) {
               stage = 0;
@@ -274,7 +282,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int item = next_active_item<MODE>(a, blockIdx.x, n_items); item < n_items && ok;) {
         const int next = next_active_item<MODE>(a, item + gridDim.x, n_items);
         const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
-        if (qb != prev_qb) {
+        if (qb != prev_qb && !a.stream_q) {
           ok = mbar_wait(q_full, qphase);
           qphase ^= 1;
           if (!ok) break;
@@ -293,7 +301,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             ok = mbar_wait(&x_full[stage], xphase);
             if (!ok) break;
             tc_fence_after();
-            const uint32_t qa = smem_u32(sq + kb * Q_BLOCK_BYTES), xa = smem_u32(sx + stage * X_STAGE_BYTES);
+            const uint32_t xa = smem_u32(sx + stage * sbytes);
+            const uint32_t qa = a.stream_q ? xa + X_STAGE_BYTES : smem_u32(sq + kb * Q_BLOCK_BYTES);
 #pragma unroll
             for (int k = 0; k < BK / 16; ++k)
               umma_bf16(dcol, smem_desc_sw128(qa + 32 * k), smem_desc_sw128(xa + 32 * k), idesc, kb > 0 || k > 0);
@@ -309,7 +318,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         if (!ok) break;
         // the query block's buffer is free for the next one once these MMAs complete
-        if (issued && next < n_items && next % a.q_blocks != qb) umma_commit(q_empty);
+        if (issued && !a.stream_q && next < n_items && next % a.q_blocks != qb) umma_commit(q_empty);
         item = next;
       }
       if (issued) {
@@ -1007,7 +1016,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   DeviceGuard g(h->device);
   cudaStream_t st = (cudaStream_t)stream;
   const bool dot_space = h->space == NMSG_SPACE_L2 || h->space == NMSG_SPACE_COSINE || h->space == NMSG_SPACE_NEGDOT;
-  if (!dot_space || ((dim + BK - 1) / BK) > KB_MAX)
+  if (!dot_space || ((dim + BK - 1) / BK) > KB_STREAM_MAX || (flags & NMSG_EXACT_SCAN))
     return scan_fallback(h, queries, nq, dim, k, kmax, ids, dists, counts, stats, dev_ptrs, st);
   if (!h->bf) {
     h->bf = new BruteForceState();
@@ -1104,7 +1113,8 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ga.chunk_tiles = s_chunk_tiles;
   ga.n_chunks = s_chunks;
   ga.q_blocks = q_blocks;
-  ga.stages = kb <= 2 ? 3 : 2;
+  ga.stream_q = kb > KB_MAX ? 1 : 0;
+  ga.stages = ga.stream_q ? 3 : (kb <= 2 ? 3 : 2);
   ga.per_column = s_tiles == n_tiles;
   ga.key_l2 = l2;
   ga.xnorm2 = s->xn.as<float>();
@@ -1115,7 +1125,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   ga.tau = s->tau.as<float>();
   ga.q_active = s->qact.as<uint8_t>();
   ga.status = s->status.as<int32_t>();
-  const int smem = SmemLayout(kb, ga.stages).total + 1024;
+  const int smem = SmemLayout(kb, ga.stages, ga.stream_q).total + 1024;
   BF_CUDA((cudaError_t)allow_max_smem((const void*)bf16_scan_kernel<0>), "smem attribute");
   BF_CUDA((cudaError_t)allow_max_smem((const void*)bf16_scan_kernel<1>), "smem attribute");
   bf16_scan_kernel<0><<<std::min(q_blocks * s_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, ga);

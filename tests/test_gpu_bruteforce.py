@@ -63,12 +63,12 @@ def test_bruteforce_matches_fp64(name, k):
 @pytest.mark.parametrize("name,k,nq", [("negdot_d960", 10, 40), ("l1_d22", 10, 50), ("l1_d64", 32, 50),
                                        ("linf_d37", 10, 50), ("linf_d128", 5, 50)])
 def test_exact_scan_matches_reference_distances(name, k, nq):
-    """L1 / LInf and rows wider than 256 take the exact CUDA-core scan: every id and distance
-    equals a full scan with the oracle's restatement of the reference's distance function
+    """L1 / LInf (and any space with exact_scan=True) take the exact CUDA-core scan: every id and
+    distance equals a full scan with the oracle's restatement of the reference's distance function
     (bit for bit), ordered by (distance, node)."""
     idx = _index(name)
     q = load_golden(name)["queries"][:nq]
-    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True)
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True, exact_scan=True)
     ix = OracleIndex(golden_path(name))
     vecs, ext, _, _ = ix.export()
     dt = ix.info["dist_type"]
@@ -85,10 +85,11 @@ def test_exact_scan_matches_reference_distances(name, k, nq):
 @pytest.mark.parametrize("space,code,dim", [("l2", 0, 307), ("l2", 0, 320), ("cosinesimil", 1, 304),
                                             ("negdotprod", 2, 271)])
 def test_exact_scan_wide_rows_tiled(tmp_path, space, code, dim):
-    """Rows wider than 256 in the fused-multiply-add spaces take the register-tiled scan: odd widths
-    (16-element half block, 4-wide and scalar tails), a row count that ends inside a warp's pass,
-    several chunks and a last query block of 4; every id and distance equals the oracle's full
-    scan bit for bit."""
+    """The exact CUDA-core scan of the fused-multiply-add spaces (the register-tiled kernel): odd
+    widths (16-element half block, 4-wide and scalar tails), a row count that ends inside a warp's
+    pass, several chunks and a last query block of 4; every id and distance equals the oracle's full
+    scan bit for bit. The same rows through the default tensor-core path (query K-blocks streamed,
+    the rows being wider than 256) give the float64 top-k ids and distances within float rounding."""
     rng = np.random.default_rng(dim)
     n, nq, k = 4_333, 20, 12
     base = rng.standard_normal((n, dim)).astype(np.float32)
@@ -97,8 +98,14 @@ def test_exact_scan_wide_rows_tiled(tmp_path, space, code, dim):
     _capi.build_index(base, code, 4, 16, nthreads=0, out_path=p)
     idx = nmslib.init(method="hnsw", space=space)
     idx.loadIndex(p)
-    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True)
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True, exact_scan=True)
     assert st[0] == 0 and st[1] == n and st[3] >= 2
+    ti, td, tc, tst = idx.bruteForceBatchArrays(q, k, stats=True)
+    assert tst[0] >= 1  # the tensor-core path
+    want_i, want_d = fp64_topk(p, q, k, space)
+    np.testing.assert_array_equal(tc, np.full(nq, k))
+    np.testing.assert_array_equal(ti, want_i)
+    np.testing.assert_allclose(td, want_d, rtol=2e-6, atol=2e-6)
     ix = OracleIndex(p)
     vecs, ext, _, _ = ix.export()
     dt = ix.info["dist_type"]
@@ -138,7 +145,7 @@ def test_exact_scan_tiled_k_extremes_and_ties(tmp_path, k):
     _capi.build_index(base, 0, 4, 16, nthreads=0, out_path=p)
     idx = nmslib.init(method="hnsw", space="l2")
     idx.loadIndex(p)
-    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True)
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True, exact_scan=True)
     assert st[0] == 0 and st[3] >= 2
     for qi, (want_i, want_d) in enumerate(_oracle_scan(p, q, k)):
         assert cnt[qi] == k
@@ -156,7 +163,7 @@ def test_exact_scan_tiled_zero_cosine_query(tmp_path):
     _capi.build_index(base, 1, 4, 16, nthreads=0, out_path=p)
     idx = nmslib.init(method="hnsw", space="cosinesimil")
     idx.loadIndex(p)
-    ids, d, cnt, st = idx.bruteForceBatchArrays(q, 10, stats=True)
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, 10, stats=True, exact_scan=True)
     want = _oracle_scan(p, q, 10, cosine=True)
     for qi, (want_i, want_d) in enumerate(want):
         np.testing.assert_array_equal(ids[qi], want_i)
@@ -222,3 +229,17 @@ def test_bruteforce_capacity_error(tmp_path):
     idx.loadIndex(p)
     with pytest.raises(RuntimeError, match="within the BF16 error bound"):
         idx.bruteForceBatchArrays(base[:2] + 0.5, 10)
+
+
+@pytest.mark.parametrize("k", [1, 10, 32])
+def test_tensor_core_wide_rows_match_fp64(k):
+    """960-wide negative dot products (the reference-built fixture) on the tensor cores with the
+    query block's K-blocks streamed beside the base's: the float64 top-k ids, ties by id."""
+    name = "negdot_d960"
+    idx = _index(name)
+    q = load_golden(name)["queries"]
+    ids, d, cnt, st = idx.bruteForceBatchArrays(q, k, stats=True)
+    assert st[0] >= 1
+    want_i, want_d = fp64_topk(golden_path(name), q, k, "negdotprod")
+    np.testing.assert_array_equal(ids[:, :k], want_i)
+    np.testing.assert_allclose(d[:, :k], want_d, rtol=2e-6, atol=2e-6)
