@@ -554,27 +554,37 @@ def fp64_truth(base, queries, k, space):
     return kth
 
 
-def run_aux(args):
+def aux_workload(which, device=0, serving_rates=(250e3, 500e3, 1e6)):
+    """One of the other benchmark configurations, measured on this GPU, as a dict:
+    c3 = 1M x 100 cosine (M 24): HNSW efSearch sweep with recall@10 against float64, the reference's
+         CPU knnQueryBatch at efSearch 200, and the tensor-core brute force of 10K queries checked
+         against float64; c4 = 1M x 960 negdot (M 16): one launch of 8K queries with per-query
+         k in {1, 10, 100} and efSearch in [64, 1024] (SearchOld at 1000 and above), the reference
+         on a sample of the same mix, and the streamed tensor-core brute force of 1K queries;
+    c5 = 5M x 96 l2 (M 32): the serving loop under open-loop Poisson arrivals of requests of
+         1-256 queries (k in {10, 100}, efSearch in {100, 400}), p50 / p99 latency.
+    Indices are built by the engine's device-assisted builder (the reference's createIndex on these
+    sizes takes minutes to tens of minutes) and cached on this machine."""
     import torch
 
     import nmslib_b200 as nmslib
     from nmslib_b200 import SPACES, _capi
-    from nmslib_b200.build import build
-    from nmslib_b200.datasets import workload
-    build()
-    name = AUX[args.workload]
-    base, queries, space, m = workload(name)
-    path = os.path.join(CACHE_DIR, f"{name}_M{m}_efc{EFC}_seed0.hnsw")
+    name = AUX[which]
+    t_start = time.time()
+    base, queries, space, m = workload_data(name)
+    path = os.path.join(CACHE_DIR, f"{name}_M{m}_efc{EFC}_device_build.hnsw")
+    build_s = None
     if not os.path.exists(path):
         os.makedirs(CACHE_DIR, exist_ok=True)
         t0 = time.time()
-        _capi.build_index(base, SPACES[space], m, EFC, nthreads=0, seed=0, out_path=path + ".tmp")
+        _capi.build_index(base, SPACES[space], m, EFC, nthreads=0, seed=0, out_path=path + ".tmp", device=device)
         os.replace(path + ".tmp", path)
-        log(f"[bench] built {path} in {time.time() - t0:.1f}s")
-    index = nmslib.init(method="hnsw", space=space)
+        build_s = round(time.time() - t0, 1)
+    index = nmslib.init(method="hnsw", space=space, device=device)
     index.loadIndex(path)
     out = {"workload": name, "n_base": len(base), "nq": len(queries), "dim": base.shape[1], "M": m,
-           "efConstruction": EFC, "space": space}
+           "efConstruction": EFC, "space": space, "index_builder": "nmslib_b200 device-assisted build",
+           "index_build_s": build_s}
 
     def timed(fn, reps=3):
         fn()
@@ -587,60 +597,105 @@ def run_aux(args):
             best = dt if best is None else min(best, dt)
         return best, r
 
-    if args.workload in ("c3", "c5"):
+    if which == "c3":
         qs = queries[:10_000]
         kth = fp64_truth(base, qs, 10, space)
         rows = []
-        for ef in ((50, 100, 200, 400) if args.workload == "c3" else (50, 100, 200, 400)):
+        for ef in (50, 100, 200, 400):
             index.setQueryTimeParams({"efSearch": ef})
             dt, (ids, d, cnt) = timed(lambda: index.knnQueryBatchArrays(qs, 10))
             rows.append({"efSearch": ef, "recall@10": round(recall_at_k(d.astype(np.float64), cnt, kth, 10), 4),
                          "qps_e2e": round(len(qs) / dt)})
             log(f"[bench] {name} ef={ef}: {rows[-1]}")
         out["hnsw"] = rows
-        ef_ref = 200 if args.workload == "c3" else 100
-        cpu = cpu_reference_qps(path, qs, ef_ref, 10, space=space)
-        out["cpu_reference"] = {"efSearch": ef_ref, "qps": round(cpu["value"]), "cores": cpu["cores"],
-                                "kind": cpu["kind"], "sample": cpu["sample"],
-                                "one_thread_qps": round(cpu["one_thread"]["value"])}
-    if args.workload == "c3":
-        out["bruteforce"] = brute_force_measure(index, queries[:10_000])
-    if args.workload == "c5":
-        out["serving"] = serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6, 2e6), workload=name)
-    if args.workload == "c4":
+        cpu = cpu_reference_qps(path, qs, 200, 10, space=space, one_thread=False)
+        out["cpu_reference"] = {"efSearch": 200, "qps": round(cpu["value"]), "cores": cpu["cores"],
+                                "kind": cpu["kind"], "sample": cpu["sample"]}
+        out["bruteforce"] = brute_force_measure(index, qs)
+        out["bruteforce"]["verify_fp64"] = bf_verify_keys(base, qs, index, space)
+    elif which == "c4":
         rng = np.random.default_rng(4)
         nq = len(queries)
         k = rng.choice([1, 10, 100], nq).astype(np.int32)
         ef = rng.integers(64, 1025, nq).astype(np.int32)
-        kth = fp64_truth(base, queries, 100, space)
         dt, (ids, d, cnt) = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
-        # recall@k per query against the float64 k-th distance of that query's own k
-        kth_k = np.array([fp for fp in kth])  # k = 100 column; per-k recall below uses the row's own k
-        out["bruteforce"] = brute_force_measure(index, queries[:1000])
-        out["mixed_batch"] = {"queries": nq, "qps_e2e": round(nq / dt), "ms": round(dt * 1e3, 2),
-                              "searchold_queries": int((ef >= 1000).sum())}
         truth10 = fp64_truth(base, queries, 10, space)
         sel = k == 10
-        out["mixed_batch"]["recall@10_of_k10_queries"] = round(
-            recall_at_k(d[sel][:, :10].astype(np.float64), cnt[sel], truth10[sel], 10), 4)
-        del kth_k
-        # reference: the same mixed batch, grouped by (k, ef) as the reference needs one ef per call
+        out["mixed_batch"] = {"queries": nq, "qps_e2e": round(nq / dt), "ms": round(dt * 1e3, 2),
+                              "searchold_queries": int((ef >= 1000).sum()),
+                              "recall@10_of_k10_queries": round(
+                                  recall_at_k(d[sel][:, :10].astype(np.float64), cnt[sel], truth10[sel], 10), 4)}
+        log(f"[bench] {name} mixed batch: {out['mixed_batch']}")
         ref = reference_module_or_none()
         if ref is not None:
-            idx = ref.init(method="hnsw", space=space)
-            idx.loadIndex(path)
+            r = ref.init(method="hnsw", space=space)
+            r.loadIndex(path)
             sample = np.arange(min(nq, 2000))
             t_total = 0.0
             for kk in (1, 10, 100):
                 for e in np.unique(ef[sample][k[sample] == kk]):
                     rows = sample[(k[sample] == kk) & (ef[sample] == e)]
-                    idx.setQueryTimeParams({"efSearch": int(e)})
+                    r.setQueryTimeParams({"efSearch": int(e)})
                     t0 = time.perf_counter()
-                    idx.knnQueryBatch(queries[rows], k=int(kk), num_threads=os.cpu_count())
+                    r.knnQueryBatch(queries[rows], k=int(kk), num_threads=os.cpu_count())
                     t_total += time.perf_counter() - t0
-            out["cpu_reference"] = {"qps": round(len(sample) / t_total), "cores": os.cpu_count(), "kind": "reference",
+            out["cpu_reference"] = {"qps": round(len(sample) / t_total), "cores": os.cpu_count(),
+                                    "kind": "reference",
                                     "sample": f"{len(sample)} queries of the mixed batch, grouped by (k, efSearch)"}
-    print(json.dumps(out))
+        out["bruteforce"] = brute_force_measure(index, queries[:1000])
+        out["bruteforce"]["verify_fp64"] = bf_verify_keys(base, queries[:1000], index, space)
+    elif which == "c5":
+        qs = queries[:10_000]
+        kth = fp64_truth(base, qs, 10, space)
+        rows = []
+        for efs in (100, 400):
+            index.setQueryTimeParams({"efSearch": efs})
+            dt, (ids, d, cnt) = timed(lambda: index.knnQueryBatchArrays(qs, 10))
+            rows.append({"efSearch": efs, "recall@10": round(recall_at_k(d.astype(np.float64), cnt, kth, 10), 4),
+                         "qps_e2e": round(len(qs) / dt)})
+            log(f"[bench] {name} ef={efs}: {rows[-1]}")
+        out["hnsw"] = rows
+        out["serving"] = serve_sweep(index, queries, rates_qps=serving_rates, workload=name)
+    del index
+    torch.cuda.empty_cache()
+    out["seconds"] = round(time.time() - t_start, 1)
+    return out
+
+
+def bf_verify_keys(base, queries, index, space, k=10):
+    """Brute-force results against float64 for any space: the float64 distances of the returned ids
+    equal the float64 top-k distances (to 1e-9 relative, the float64 sums of the two being in
+    different orders), and the fraction of queries whose sets agree that way."""
+    import torch
+    ids, d, cnt = index.bruteForceBatchArrays(queries, k)
+    b = torch.from_numpy(base).cuda().double()
+    if space == "cosinesimil":
+        b = b / b.norm(dim=1, keepdim=True).clamp_min(1e-300)
+    bsq = (b * b).sum(1)
+    ok = 0
+    for s0 in range(0, len(queries), 256):
+        q = torch.from_numpy(queries[s0:s0 + 256]).cuda().double()
+        if space == "cosinesimil":
+            q = q / q.norm(dim=1, keepdim=True).clamp_min(1e-300)
+            full = 1 - q @ b.T
+        elif space == "negdotprod":
+            full = -(q @ b.T)
+        else:
+            full = (q * q).sum(1, keepdim=True) - 2 * q @ b.T + bsq[None, :]
+        top, _ = torch.topk(full, k, dim=1, largest=False)
+        got = torch.gather(full, 1, torch.from_numpy(ids[s0:s0 + 256, :k].astype(np.int64)).cuda())
+        got, _ = torch.sort(got, dim=1)
+        tol = 1e-9 * top.abs().clamp_min(1.0)
+        ok += int(((got - top).abs() <= tol).all(dim=1).sum().item())
+    del b
+    torch.cuda.empty_cache()
+    return {"queries": len(queries), "exact_topk_frac": ok / max(1, len(queries))}
+
+
+def run_aux(args):
+    from nmslib_b200.build import build
+    build()
+    print(json.dumps(aux_workload(args.workload)))
 
 
 # ------------------------------------------------------------------ main
@@ -657,6 +712,8 @@ def main():
     ap.add_argument("--profile-scan", type=int, default=0, metavar="N",
                     help="profiling run: the exact CUDA-core scan alone (200 queries, k=10) over N x 960 normal "
                          "rows (negdot, a small device-built graph), warmup + steps calls")
+    ap.add_argument("--no-aux", action="store_true",
+                    help="skip the c3 / c4 / c5 sections of the default line")
     ap.add_argument("--workload", choices=["c2", "c3", "c4", "c5"], default="c2",
                     help="c2 (default, the headline line); c3 cosine 1M x 100 + brute force; c4 negdot "
                          "1M x 960 mixed k/ef batch; c5 l2 5M x 96 serving")
@@ -833,6 +890,19 @@ def main():
     # ---- the index built again with the construction searches on the GPU
     build_info = build_compare(base, space, m, queries, kth, head["recall@10"], local) if world == 1 else None
 
+    # ---- the other configurations (cosine + brute force, wide mixed batch, 5M serving)
+    aux = None
+    if world == 1 and not args.no_aux:
+        del index
+        torch.cuda.empty_cache()
+        aux = {}
+        for which in ("c3", "c4", "c5"):
+            try:
+                aux[which] = aux_workload(which, local)
+            except Exception as e:  # noqa: BLE001 - reported in the line, the headline stands
+                aux[which] = {"error": f"{type(e).__name__}: {e}"}
+                log(f"[bench] {which} failed: {e}")
+
     peak, peak_kind = peaks()
     achieved = alg_bytes / (ms * 1e-3) / 1e9
     traffic = recorded_traffic()
@@ -865,7 +935,8 @@ def main():
                            "cuda_graph": True},
                 "serving": serving,
                 "bruteforce": brute,
-                "index_build": build_info}
+                "index_build": build_info,
+                "aux": aux}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
