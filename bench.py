@@ -357,13 +357,14 @@ def cpu_reference_qps(path, queries, ef, k, target_seconds=3.0, space="l2", one_
 # ------------------------------------------------------------------ serving and brute force
 def serve_sweep(index, queries, rates_qps=(250e3, 500e3, 1e6), seconds=1.0, seed=11, workload=WORKLOAD):
     """p50/p99 request latency and achieved QPS of the continuous-batching server at several
-    offered loads (queries per second), open-loop Poisson arrivals. The memory budget holds 32
-    lanes of 256 query slots (one visited byte per base vector each)."""
+    offered loads (queries per second), open-loop Poisson arrivals. The memory budget holds 32 x 256
+    search slots (one visited byte per base vector each) shared by 64 lanes; a request takes one
+    slot per query."""
     from nmslib_b200.serving import Server
     rng = np.random.default_rng(seed)
     n = index.info["n"]
     budget = max(8 << 30, int(32 * 256 * ((n + 15) // 16 * 16 + 1) * 1.05))
-    srv = Server(index, memory_budget_bytes=budget, max_batch=256, max_k=100, max_lanes=32)
+    srv = Server(index, memory_budget_bytes=budget, max_batch=256, max_k=100, max_lanes=64)
     out = []
     try:
         for qps in rates_qps:

@@ -237,10 +237,12 @@ NMSG_API int nmsg_bruteforce_knn(nmsg_index* index, const float* queries, int64_
 
 /* ---- Serving: continuous batching over a loaded index (no reference counterpart; per-request
  * semantics are knnQueryBatch's, python_bindings/nmslib.cc:142-168). Requests of 1..max_batch
- * queries, each with its own k (<= max_k) and efSearch (< 1000, V1Merge), are admitted into
- * lanes (a stream plus a fixed share of search slots) as lanes free up; the number of lanes is
- * what memory_budget_bytes allows (at most max_lanes). Requests in different lanes run
- * concurrently on the device; each request's results do not depend on the others. */
+ * queries, each with its own k (<= max_k) and efSearch (< 1000, V1Merge), are admitted oldest
+ * first as device memory frees up: a request takes one search slot per query (up to max_batch,
+ * in whole blocks of 4) from a pool that memory_budget_bytes sizes (one slot = one visited byte
+ * per stored element), and one of max_lanes lanes (a stream with staging buffers). Requests in
+ * different lanes run concurrently on the device; each request's results do not depend on the
+ * others. */
 typedef struct nmsg_server nmsg_server;
 
 NMSG_API int nmsg_server_create(nmsg_index* index, int64_t memory_budget_bytes, int32_t max_batch, int32_t max_k,

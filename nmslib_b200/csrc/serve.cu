@@ -1,13 +1,15 @@
 // Continuous-batching query server over a loaded index (the serving front of the HNSW query path).
 //
-// Requests (a batch of 1..max_batch queries with its own k and efSearch) are admitted into
-// "lanes" as soon as one is free. A lane is a CUDA stream plus a fixed share of the search
-// slots (per-warp visited-set epoch bytes) and its own staging buffers; the number of lanes is
-// what the device-memory budget allows. Every admitted request is one launch of the persistent
-// search kernel on its lane's stream, so requests that arrive while others run are searched
-// concurrently on the device, each on its own slots; nothing a request computes depends on the
-// others, so its results are the same alone and in any mix. A worker thread admits requests
-// and harvests finished lanes (event query); callers submit and wait without blocking the GPU.
+// Requests (a batch of 1..max_batch queries with its own k and efSearch) are admitted as device
+// memory frees up: each needs a run of search slots (a slot is one warp's visited-set epoch bytes,
+// the memory that grows with the index) from a pool sized by the memory budget, one slot per
+// query up to a block-rounded cap, and a lane (a CUDA stream with staging buffers; lanes are
+// cheap). Admission is first come, first served: the oldest waiting request starts as soon as its
+// slots and a lane are free. Every admitted request is one launch of the persistent search
+// kernel on its lane's stream over its own slots, so requests that arrive while others run are
+// searched concurrently on the device; nothing a request computes depends on the others, so its
+// results are the same alone and in any mix. A worker thread admits requests and harvests
+// finished lanes (event query); callers submit and wait without blocking the GPU.
 //
 // The reference has no server on this path (its Thrift front end, query_server/, is out of
 // scope); per-request semantics are those of knnQueryBatch (python_bindings/nmslib.cc:142-168).
@@ -58,6 +60,7 @@ struct Lane {
   int32_t* s_pin = nullptr;
   int64_t req = -1;
   int k = 0;
+  int slot0 = 0, nslots = 0;  // the request's run of pool slots
 };
 
 }  // namespace
@@ -65,7 +68,9 @@ struct Lane {
 struct nmsg_server {
   nmsg_index* h = nullptr;
   int max_batch = 256, max_k = 100;
-  int lane_slots = 0;
+  int pool_slots = 0;        // search slots the memory budget holds
+  int slot_cap = 0;          // most slots one request takes (its batch, rounded to whole blocks)
+  std::vector<uint8_t> slot_used;  // per block of kWarpsPerBlock slots
   int64_t vpitch = 0;
   DevBuf visited, epochs;
   std::vector<Lane> lanes;
@@ -129,9 +134,9 @@ struct nmsg_server {
     a.ids = l.ids.as<int32_t>();
     a.dists = l.dists.as<float>();
     a.counts = l.counts.as<int32_t>();
-    a.visited = visited.as<uint8_t>() + (int64_t)li * lane_slots * vpitch;
+    a.visited = visited.as<uint8_t>() + (int64_t)l.slot0 * vpitch;
     a.visited_pitch = vpitch;
-    a.epochs = epochs.as<uint8_t>() + (int64_t)li * lane_slots;
+    a.epochs = epochs.as<uint8_t>() + l.slot0;
     a.work_counter = l.counter.as<int32_t>();
     a.status = l.status.as<int32_t>();
     a.region_items = plan.region;
@@ -140,9 +145,8 @@ struct nmsg_server {
     a.stage_rows = plan.stage_rows;
     a.warp_smem = plan.warp_smem;
     a.lean = plan.lean ? 1 : 0;
-    const int wpb = plan.wpb;
-    int blocks = std::min((r.nq + wpb - 1) / wpb, lane_slots / wpb);
-    if (blocks < 1) blocks = 1;
+    const int wpb = plan.wpb;  // <= kWarpsPerBlock: the run holds whole blocks
+    const int blocks = std::max(1, l.nslots / wpb);
     a.num_slots = blocks * wpb;
     rc = launch_search(a, false, plan.gather, false, blocks, wpb, l.st);
     if (rc != 0) return NMSG_ERR_DEVICE;
@@ -156,6 +160,22 @@ struct nmsg_server {
     l.req = r.id;
     l.k = r.k;
     return NMSG_OK;
+  }
+
+  // First run of `n` free slot blocks (mu held); its first block, or -1.
+  int take_blocks(int n) {
+    int run = 0;
+    for (int b = 0; b < (int)slot_used.size(); ++b) {
+      run = slot_used[b] ? 0 : run + 1;
+      if (run == n) {
+        for (int t = b - n + 1; t <= b; ++t) slot_used[t] = 1;
+        return b - n + 1;
+      }
+    }
+    return -1;
+  }
+  void give_blocks(int b0, int n) {
+    for (int t = b0; t < b0 + n; ++t) slot_used[t] = 0;
   }
 
   void run() {
@@ -179,23 +199,37 @@ struct nmsg_server {
         r.q.shrink_to_fit();
         r.done = true;
         l.req = -1;
+        give_blocks(l.slot0 / kWarpsPerBlock, l.nslots / kWarpsPerBlock);
         --in_flight;
         progressed = true;
       }
       if (progressed) cv_done.notify_all();
-      // admit waiting requests into free lanes
-      for (size_t li = 0; li < lanes.size() && !queue.empty(); ++li) {
-        if (lanes[li].req >= 0) continue;
+      // admit waiting requests, oldest first, while a lane and a run of slots are free
+      while (!queue.empty()) {
+        int li = -1;
+        for (size_t t = 0; t < lanes.size(); ++t)
+          if (lanes[t].req < 0) {
+            li = (int)t;
+            break;
+          }
+        if (li < 0) break;
         Request& r = reqs[queue.front()];
+        const int need_blocks = (std::min(r.nq, slot_cap) + kWarpsPerBlock - 1) / kWarpsPerBlock;
+        const int b0 = take_blocks(need_blocks);
+        if (b0 < 0) break;  // the oldest request waits for memory
         queue.pop_front();
+        Lane& l = lanes[li];
+        l.slot0 = b0 * kWarpsPerBlock;
+        l.nslots = need_blocks * kWarpsPerBlock;
         ++in_flight;
-        const int rc = launch((int)li, r);
+        const int rc = launch(li, r);
         if (rc != NMSG_OK) {
           r.status = rc;
           r.done = true;
           r.t_done = now_s();
           --in_flight;
-          lanes[li].req = -1;
+          l.req = -1;
+          give_blocks(l.slot0 / kWarpsPerBlock, l.nslots / kWarpsPerBlock);
           cv_done.notify_all();
         }
         progressed = true;
@@ -237,18 +271,26 @@ NMSG_API int nmsg_server_create(nmsg_index* h, int64_t memory_budget_bytes, int3
   s->max_batch = max_batch;
   s->max_k = max_k;
   s->vpitch = ((d.n + 15) / 16) * 16;
-  // slots per lane: one warp per query of the largest batch, in whole blocks
-  s->lane_slots = ((max_batch + kWarpsPerBlock - 1) / kWarpsPerBlock) * kWarpsPerBlock;
-  const int64_t per_lane = (int64_t)s->lane_slots * (s->vpitch + 1) + (int64_t)max_batch * (d.dim * 4 + max_k * 8 + 8);
-  int nlanes = (int)std::min<int64_t>(max_lanes, memory_budget_bytes / per_lane);
-  if (nlanes < 1) {
+  // a request takes one slot per query up to its batch, in whole blocks; the lanes' staging comes
+  // off the budget first, the slots share the rest
+  s->slot_cap = ((max_batch + kWarpsPerBlock - 1) / kWarpsPerBlock) * kWarpsPerBlock;
+  const int64_t per_lane = (int64_t)max_batch * (d.dim * 4 + max_k * 8 + 8);
+  const int nlanes = max_lanes;
+  const int64_t slot_bytes = memory_budget_bytes - (int64_t)nlanes * per_lane;
+  const int64_t slots = slot_bytes > 0 ? slot_bytes / (s->vpitch + 1) : 0;
+  s->pool_slots = (int)std::min<int64_t>(slots / kWarpsPerBlock * kWarpsPerBlock, 1 << 20);
+  if (s->pool_slots < kWarpsPerBlock) {
     delete s;
-    return srv_fail(NMSG_ERR_OOM, "the memory budget does not hold one lane (" + std::to_string(per_lane) + " bytes)");
+    return srv_fail(NMSG_ERR_OOM, "the memory budget does not hold the lanes and one block of search slots (" +
+                                      std::to_string((int64_t)nlanes * per_lane + kWarpsPerBlock * (s->vpitch + 1)) +
+                                      " bytes)");
   }
+  s->slot_cap = std::min(s->slot_cap, s->pool_slots);
+  s->slot_used.assign(s->pool_slots / kWarpsPerBlock, 0);
   DeviceGuard g(h->device);
   int rc = NMSG_OK;
-  if (s->visited.ensure((size_t)nlanes * s->lane_slots * s->vpitch, true) != cudaSuccess ||
-      s->epochs.ensure((size_t)nlanes * s->lane_slots, true) != cudaSuccess)
+  if (s->visited.ensure((size_t)s->pool_slots * s->vpitch, true) != cudaSuccess ||
+      s->epochs.ensure((size_t)s->pool_slots, true) != cudaSuccess)
     rc = NMSG_ERR_OOM;
   s->lanes.resize(nlanes);
   for (Lane& l : s->lanes) {

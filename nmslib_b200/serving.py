@@ -5,9 +5,10 @@
     ids, dists, counts, latency = srv.wait(rid)  # ids/dists are [nq, k]
     lat, wall = srv.run_trace(pool, offsets, sizes, ks, efs, arrivals)   # open-loop replay
 
-Requests are admitted into lanes (a CUDA stream plus a share of search slots) as lanes free up;
-the lane count is bounded by the memory budget. Requests in different lanes run concurrently
-on the GPU and each request's results are independent of the others.
+Requests are admitted oldest first as device memory frees up: each takes one search slot per
+query (the visited-set bytes; up to max_batch) from a pool the memory budget sizes, and one of
+max_lanes lanes (a CUDA stream with staging). Requests in different lanes run concurrently on the
+GPU and each request's results are independent of the others.
 """
 from __future__ import annotations
 

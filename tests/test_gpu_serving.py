@@ -73,3 +73,28 @@ def test_rejects_bad_requests(served):
         srv.submit(q[:4], 101, 50)     # above max_k
     with pytest.raises(RuntimeError):
         srv.submit(q[:4], 10, 1000)    # SearchOld is not served
+
+
+def test_admission_waits_for_memory():
+    """A budget that holds the slots of one full request only (64 slots of 10K visited bytes,
+    besides the lanes' staging): requests wait for memory rather than for a lane, all complete,
+    and each result is the plain batch search's."""
+    idx = nmslib.init(method="hnsw", space="l2")
+    idx.loadIndex(golden_path("c1_l2_d128"))
+    lane_staging = 64 * (128 * 4 + 100 * 8 + 8)
+    budget = 8 * lane_staging + 64 * (10_000 + 1) + 100
+    srv = Server(idx, memory_budget_bytes=budget, max_batch=64, max_k=100, max_lanes=8)
+    try:
+        q = load_golden("c1_l2_d128")["queries"]
+        reqs = _requests(len(q))
+        rids = [srv.submit(q[s:s + b], k, ef) for s, b, k, ef in reqs]
+        for (s, b, k, ef), rid in zip(reqs, rids):
+            got = srv.wait(rid)[:3]
+            idx.setQueryTimeParams({"efSearch": ef})
+            bi, bd, bc = idx.knnQueryBatchArrays(q[s:s + b], k)
+            np.testing.assert_array_equal(got[0], bi)
+            np.testing.assert_array_equal(got[2], bc)
+    finally:
+        srv.close()
+    with pytest.raises(MemoryError):
+        Server(idx, memory_budget_bytes=8 * lane_staging, max_batch=64, max_k=100, max_lanes=8)
