@@ -706,7 +706,8 @@ __global__ void rerank_kernel(RerankArgs a) {
 namespace nmsg {
 
 struct BruteForceState {
-  int kp = 0;       // padded dim (multiple of 64, <= 256)
+  bool base_ready = false;  // the BF16 base and its bounds exist (the exact scan needs none of it)
+  int kp = 0;       // padded dim (multiple of 64, <= 4096)
   float max_xn = 0; // largest |x|^2 over the base (l2 bound)
   DevBuf x16, x32, xn, xn_hi, xn_lo, xt_max, dx_max;
   DevBuf q32, q16, qn_hi, qn_lo, eps, cand_key, cand_id, cand_cnt, tau, needs, qact, coll_id, coll_key, coll_cnt, found;
@@ -875,6 +876,9 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // 2-D bf16 tensor map over a [rows][kp] matrix, 64 x box_rows tiles with the 128-byte swizzle.
+// The driver's result code of the last failed encoding (for the error message).
+thread_local int g_tmap_result = 0;
+
 bool make_tmap(CUtensorMap* m, void* base, int64_t rows, int kp, int box_rows) {
   auto enc = tensor_map_encoder();
   if (!enc) return false;
@@ -882,9 +886,17 @@ bool make_tmap(CUtensorMap* m, void* base, int64_t rows, int kp, int box_rows) {
   cuuint64_t strides[1] = {(cuuint64_t)kp * 2};
   cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  g_tmap_result = (int)r;
+  return r == CUDA_SUCCESS;
+}
+
+std::string tmap_error(const char* what, int64_t rows, int kp, const void* base) {
+  return std::string("cuTensorMapEncodeTiled (") + what + "): CUresult " + std::to_string(g_tmap_result) +
+         ", rows " + std::to_string(rows) + ", padded dim " + std::to_string(kp) + ", address " +
+         std::to_string((uintptr_t)base % 1024) + " mod 1024";
 }
 
 int bf_fail(int code, const std::string& msg) {
@@ -933,7 +945,7 @@ int prepare_base(nmsg_index* h, BruteForceState* s) {
     BF_CUDA(cudaMemcpy(s->xn.as<float>() + n, inf.data(), inf.size() * 4, cudaMemcpyHostToDevice), "pad norms");
   }
   BF_CUDA(cudaDeviceSynchronize(), "prepare base");
-  if (!make_tmap(&s->tmx, s->x16.p, n, s->kp, BN)) return bf_fail(NMSG_ERR_DEVICE, "cuTensorMapEncodeTiled (base)");
+  if (!make_tmap(&s->tmx, s->x16.p, n, s->kp, BN)) return bf_fail(NMSG_ERR_DEVICE, tmap_error("base", n, s->kp, s->x16.p));
   return NMSG_OK;
 }
 
@@ -1018,14 +1030,15 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   const bool dot_space = h->space == NMSG_SPACE_L2 || h->space == NMSG_SPACE_COSINE || h->space == NMSG_SPACE_NEGDOT;
   if (!dot_space || ((dim + BK - 1) / BK) > KB_STREAM_MAX || (flags & NMSG_EXACT_SCAN))
     return scan_fallback(h, queries, nq, dim, k, kmax, ids, dists, counts, stats, dev_ptrs, st);
-  if (!h->bf) {
-    h->bf = new BruteForceState();
+  if (!h->bf) h->bf = new BruteForceState();
+  if (!h->bf->base_ready) {
     const int rc = prepare_base(h, h->bf);
     if (rc != NMSG_OK) {
       destroy_bruteforce(h->bf);
       h->bf = nullptr;
       return rc;
     }
+    h->bf->base_ready = true;
   }
   BruteForceState* s = h->bf;
   const int kp = s->kp, kb = kp / BK;
@@ -1099,7 +1112,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
                                                      s->qn_lo.as<float>(), s->eps.as<float>());
   BF_CUDA(cudaGetLastError(), "prepare queries");
   CUtensorMap tmq;
-  if (!make_tmap(&tmq, s->q16.p, mpad, kp, BM)) return bf_fail(NMSG_ERR_DEVICE, "cuTensorMapEncodeTiled (queries)");
+  if (!make_tmap(&tmq, s->q16.p, mpad, kp, BM)) return bf_fail(NMSG_ERR_DEVICE, tmap_error("queries", mpad, kp, s->q16.p));
   BF_CUDA(cudaMemsetAsync(s->status.p, 0, 4, st), "reset status");
 
   // 1. top-CAND BF16 candidates of the sample, exact rerank -> tau

@@ -243,3 +243,19 @@ def test_tensor_core_wide_rows_match_fp64(k):
     want_i, want_d = fp64_topk(golden_path(name), q, k, "negdotprod")
     np.testing.assert_array_equal(ids[:, :k], want_i)
     np.testing.assert_allclose(d[:, :k], want_d, rtol=2e-6, atol=2e-6)
+
+
+def test_exact_scan_then_tensor_path_on_one_index():
+    """The exact scan first, then the tensor-core path, then the exact scan again on the same
+    loaded index: each call prepares what it needs and gives its own path's results."""
+    name = "c1_l2_d128"
+    idx = _index(name)
+    q = load_golden(name)["queries"][:30]
+    want_i, want_d = fp64_topk(golden_path(name), q, 10, "l2")
+    a = idx.bruteForceBatchArrays(q, 10, stats=True, exact_scan=True)
+    b = idx.bruteForceBatchArrays(q, 10, stats=True)
+    c = idx.bruteForceBatchArrays(q, 10, stats=True, exact_scan=True)
+    assert a[3][0] == 0 and b[3][0] >= 1 and c[3][0] == 0
+    np.testing.assert_array_equal(b[0], want_i)
+    np.testing.assert_array_equal(a[0], c[0])
+    np.testing.assert_array_equal(a[1].view(np.int32), c[1].view(np.int32))
