@@ -218,6 +218,9 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
     if (p.ctx > 1)
       p.bulk_rows = cfg.row_copy == 2 || (cfg.row_copy == 0 && d.dim * 4 >= kBulkRowMinBytes);
   }
+  // the general kernels stage wide rows with one bulk copy each (row_copy 2 asks for it always)
+  if (p.gather == 0 && p.ctx == 1)
+    p.bulk_rows = cfg.row_copy == 2 || (cfg.row_copy == 0 && d.dim * 4 >= kBulkRowMinBytes);
   // the lean kernel: V1Merge with one query per warp over the index shapes it is compiled for,
   // rows staged by bulk copies (row_copy 1 asks for the 16-byte copies of the general kernel)
   p.lean = false;

@@ -524,6 +524,7 @@ int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int
   a.stage_rows = plan.stage_rows;
   a.warp_smem = plan.warp_smem;
   a.lean = plan.lean ? 1 : 0;
+  a.bulk_rows = plan.bulk_rows ? 1 : 0;
 
   std::vector<float> hq((size_t)max_batch * dim);
   std::vector<int32_t> hids((size_t)max_batch * efc), hcnt(max_batch);

@@ -307,22 +307,40 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // Distances to rows ids[0..n) through the warp's staging area: each round copies up to
 // `stage_rows` rows into shared memory with asynchronous 16-byte copies (every row of the round
 // in flight at once, no registers held), then the four 8-lane groups reduce them.
+// With `bar` set, each row is one bulk copy (TMA unit) issued by one lane and completing on that
+// mbarrier (phase in *phase); a copy that does not complete within the wait bound sets *failed.
 __device__ void compute_dists_staged(const DevIndex& ix, const float* __restrict__ q, const int* __restrict__ ids,
-                                     int n, float* __restrict__ out, float* __restrict__ stage, int stage_rows) {
+                                     int n, float* __restrict__ out, float* __restrict__ stage, int stage_rows,
+                                     uint64_t* bar, uint32_t* phase, bool* failed) {
   const int lane = lane_id();
   const int g = lane >> 3, j = lane & 7;
   const int nf4 = (ix.dim + 3) >> 2;  // 16-byte chunks covering elements [0, dim)
   const int nfull = ix.n16 >> 5;
   const bool half = (ix.n16 & 31) != 0;
   const int code = ix.dist_type;
+  const uint32_t row_bytes = (uint32_t)bulk_row_bytes(ix);
   for (int base = 0; base < n; base += stage_rows) {
     const int cnt = min(stage_rows, n - base);
-    for (int r = 0; r < cnt; ++r) {
-      const float* src = ix.vecs + (int64_t)ids[base + r] * ix.pitch;
-      float* dst = stage + r * ix.pitch;
-      for (int c = lane; c < nf4; c += 32) cp_async16(dst + 4 * c, src + 4 * c);
+    if (bar) {
+      if (lane == 0) sm100::mbar_arrive_expect_tx(bar, (uint32_t)cnt * row_bytes);
+      __syncwarp();
+      for (int r = lane; r < cnt; r += 32) {
+        sm100::fence_proxy_async_smem();
+        sm100::bulk_copy_g2s(stage + r * ix.pitch, ix.vecs + (int64_t)ids[base + r] * ix.pitch, row_bytes, bar);
+      }
+      if (!sm100::mbar_wait(bar, *phase)) {
+        sm100::mbar_wait(bar, *phase);  // bounded: no copy may be left writing the staging rows
+        *failed = true;
+      }
+      *phase ^= 1;
+    } else {
+      for (int r = 0; r < cnt; ++r) {
+        const float* src = ix.vecs + (int64_t)ids[base + r] * ix.pitch;
+        float* dst = stage + r * ix.pitch;
+        for (int c = lane; c < nf4; c += 32) cp_async16(dst + 4 * c, src + 4 * c);
+      }
+      cp_async_wait_all();
     }
-    cp_async_wait_all();
     __syncwarp();
     for (int r0 = 0; r0 < cnt; r0 += 4) {
       const int r = r0 + g;
@@ -421,6 +439,9 @@ struct WarpCtx {
   float* sk;     // [nbpad]
   int* sv;       // [nbpad]
   float* stage;  // staged-gather rows (stage_rows x pitch), or null
+  uint64_t* bar; // bulk row copies: the warp's mbarrier (after the staging rows), or null
+  uint32_t phase;
+  bool failed;   // a bulk copy did not complete within the wait bound
   int* htab;     // shared-memory visited table (open addressing, -1 = empty), or null
   uint8_t* vis;  // HBM epoch bytes of this warp's slot
   uint8_t epoch;
@@ -567,9 +588,9 @@ __device__ int expand_list(WarpCtx& w, const int32_t* lst, int maxcnt, int* cnt_
 }
 
 template <int G>
-__device__ __forceinline__ void dists(const SearchArgs& a, const WarpCtx& w, const int* ids, int n, float* out) {
+__device__ __forceinline__ void dists(const SearchArgs& a, WarpCtx& w, const int* ids, int n, float* out) {
   if (G == 0)
-    compute_dists_staged(a.ix, w.q, ids, n, out, w.stage, a.stage_rows);
+    compute_dists_staged(a.ix, w.q, ids, n, out, w.stage, a.stage_rows, w.bar, &w.phase, &w.failed);
   else
     compute_dists<(G > 0 ? G : 1)>(a.ix, w.q, ids, n, out);
 }
@@ -809,6 +830,17 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
     __syncwarp();
   }
   w.stage = reinterpret_cast<float*>(tail);
+  w.bar = nullptr;
+  w.phase = 0;
+  w.failed = false;
+  if (a.bulk_rows && a.stage_rows > 0) {
+    w.bar = reinterpret_cast<uint64_t*>(w.stage + (size_t)a.stage_rows * ix.pitch);
+    if (lane == 0) {
+      sm100::mbar_init(w.bar, 1);  // idle between queries: every copy was waited for
+      sm100::fence_barrier_init();
+    }
+    __syncwarp();
+  }
 
   // next epoch of this slot's visited array; clear it when the byte wraps (hnsw.h:582-589)
   int ep = 0;
@@ -835,6 +867,10 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
     search_old<R>(a, w, qi, k, ef, cur, curdist, a.old_heap + (int64_t)slot * a.old_heap_cap);
   } else {
     search_v1merge<R>(a, w, qi, k, ef, cur, curdist);
+  }
+  if (w.failed && lane == 0) {  // a row copy gave up: the query's results are not trusted
+    set_status(a.status, NMSG_ERR_TIMEOUT);
+    a.counts[qi] = 0;
   }
   if (a.stats && lane == 0) {
     a.stats[qi * 4 + 0] = w.st_dist;
@@ -1901,7 +1937,7 @@ int multi_warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int s
 
 int warp_smem_bytes(const DevIndex& ix, int region_items, int nbpad, int hash_log2, int stage_rows) {
   int bytes = ix.pitch * 4 + region_items * 8 + nbpad * 16 + (hash_log2 > 0 ? (4 << hash_log2) : 0) +
-              stage_rows * ix.pitch * 4;
+              stage_rows * ix.pitch * 4 + (stage_rows > 0 ? 16 : 0);  // + the bulk-copy mbarrier
   return (bytes + 15) & ~15;
 }
 

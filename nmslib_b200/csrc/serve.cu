@@ -145,6 +145,7 @@ struct nmsg_server {
     a.stage_rows = plan.stage_rows;
     a.warp_smem = plan.warp_smem;
     a.lean = plan.lean ? 1 : 0;
+    a.bulk_rows = plan.bulk_rows ? 1 : 0;
     const int wpb = plan.wpb;  // <= kWarpsPerBlock: the run holds whole blocks
     const int blocks = std::max(1, l.nslots / wpb);
     a.num_slots = blocks * wpb;

@@ -295,3 +295,26 @@ def test_queries_per_warp_mixed_k_ef():
     np.testing.assert_array_equal(ids, oi)
     np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
     np.testing.assert_array_equal(st, ost)
+
+
+@pytest.mark.parametrize("stage", [3, 8, 40])
+@pytest.mark.parametrize("name,si", [("negdot_d960", 0), ("negdot_d960", 2), ("cos_d100", 1), ("l1_d22", 1),
+                                     ("c1_l2_d128", 5), ("sift_l2_ties", 2)])
+def test_bulk_row_copies_in_the_general_kernel(name, si, stage):
+    """The single-query kernels (SearchOld batches, L1 / LInf, shapes without a lean kernel, the
+    plain kernel) with each staged row fetched by one bulk copy: the oracle's results and counts."""
+    k, ef, algo = golden_manifest()[name]["settings"][si]
+    q = load_golden(name)["queries"]
+    idx = _gpu_index(name)
+    idx.setLaunchConfig(stage_rows=stage, row_copy=2)
+    try:
+        idx.setQueryTimeParams({"efSearch": ef, "algoType": algo})
+        oi, od, oc, ost = _oracle(name).search(q, k=k, ef=ef, algo=ALGO_CODES[algo])
+        for plain in (False, True):
+            ids, d, cnt, st = idx.knnQueryBatchArrays(q, k, plain=plain, stats=True)
+            np.testing.assert_array_equal(cnt, oc)
+            np.testing.assert_array_equal(ids, oi)
+            np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
+            np.testing.assert_array_equal(st, ost)
+    finally:
+        idx.setLaunchConfig()
