@@ -620,9 +620,15 @@ def aux_workload(which, device=0, serving_rates=(250e3, 500e3, 1e6)):
         k = rng.choice([1, 10, 100], nq).astype(np.int32)
         ef = rng.integers(64, 1025, nq).astype(np.int32)
         dt, (ids, d, cnt) = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
+        # the same launch with the 3840-byte rows staged by 16-byte copies spread over the lanes
+        # instead of one bulk copy per row (the default for rows of 1 KB and more)
+        index.setLaunchConfig(row_copy=1)
+        dt16, _ = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
+        index.setLaunchConfig()
         truth10 = fp64_truth(base, queries, 10, space)
         sel = k == 10
         out["mixed_batch"] = {"queries": nq, "qps_e2e": round(nq / dt), "ms": round(dt * 1e3, 2),
+                              "row_copy": {"bulk_ms": round(dt * 1e3, 2), "cp16_ms": round(dt16 * 1e3, 2)},
                               "searchold_queries": int((ef >= 1000).sum()),
                               "recall@10_of_k10_queries": round(
                                   recall_at_k(d[sel][:, :10].astype(np.float64), cnt[sel], truth10[sel], 10), 4)}
