@@ -167,6 +167,18 @@ int space_matches(int space, int dist_type) {
 
 namespace nmsg {
 
+// Rows per staging round when every row is one bulk copy completing on the warp's mbarrier: at most
+// kBulkRoundBytes per round (one mbarrier phase). Measured on B200: rounds of 30,720 bytes (8 rows
+// of 960 floats) complete; rounds of 122,880 and 153,600 bytes ran out of the wait bound and the
+// kernel reported NMSG_ERR_TIMEOUT, with the device still answering. The cause is not established,
+// so larger rounds are not issued. Returns whether *rows changed.
+static bool cap_bulk_round(const DevIndex& d, int* rows) {
+  const int cap = std::max(1, kBulkRoundBytes / bulk_row_bytes(d));
+  if (*rows <= cap) return false;
+  *rows = cap;
+  return true;
+}
+
 int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bool with_old, bool plain,
                 LaunchPlan* out, std::string* err) {
   LaunchPlan p;
@@ -215,22 +227,31 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
         break;
       }
     }
-    if (p.ctx > 1)
+    if (p.ctx > 1) {
       p.bulk_rows = cfg.row_copy == 2 || (cfg.row_copy == 0 && d.dim * 4 >= kBulkRowMinBytes);
+      if (p.bulk_rows && cap_bulk_round(d, &p.stage_rows))
+        p.warp_smem = multi_warp_smem_bytes(d, p.region, p.nbpad, p.stage_rows, p.ctx);
+    }
   }
   // the general kernels stage wide rows with one bulk copy each (row_copy 2 asks for it always)
-  if (p.gather == 0 && p.ctx == 1)
+  if (p.gather == 0 && p.ctx == 1) {
     p.bulk_rows = cfg.row_copy == 2 || (cfg.row_copy == 0 && d.dim * 4 >= kBulkRowMinBytes);
+    if (p.bulk_rows && cap_bulk_round(d, &p.stage_rows))
+      p.warp_smem = warp_smem_bytes(d, p.region, p.nbpad, p.hash_log2, p.stage_rows);
+  }
   // the lean kernel: V1Merge with one query per warp over the index shapes it is compiled for,
   // rows staged by bulk copies (row_copy 1 asks for the 16-byte copies of the general kernel)
   p.lean = false;
   if (!plain && !with_old && p.gather == 0 && p.hash_log2 == 0 && p.ctx == 1 && cfg.row_copy != 1 &&
       lean_supported(d)) {
     const int nbpad = std::max(32, ((std::max(d.maxM, d.maxM0) + 31) / 32) * 32);
-    const int ws = lean_smem_bytes(d, p.region, nbpad, p.stage_rows);
+    int rows = p.stage_rows;
+    cap_bulk_round(d, &rows);  // the lean kernel stages every row by bulk copy
+    const int ws = lean_smem_bytes(d, p.region, nbpad, rows);
     if (ws <= kMaxSmemPerBlock) {
       p.lean = true;
       p.nbpad = nbpad;
+      p.stage_rows = rows;
       p.warp_smem = ws;
     }
   }

@@ -23,6 +23,8 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kDefaultQueriesPerWarp = 1;
 // Rows wider than this many bytes are staged with one bulk copy each unless configured otherwise.
 constexpr int kBulkRowMinBytes = 1024;
+// Bytes of bulk row copies one staging round waits for on one mbarrier phase (plan_launch).
+constexpr int kBulkRoundBytes = 32768;
 constexpr int kMaxSmemPerBlock = 227 * 1024;
 
 // Launch shape of one search launch (see plan_launch).
