@@ -240,16 +240,17 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
       p.warp_smem = warp_smem_bytes(d, p.region, p.nbpad, p.hash_log2, p.stage_rows);
   }
   // the lean kernel: V1Merge with one query per warp over the index shapes it is compiled for,
-  // rows staged by bulk copies (row_copy 1 asks for the 16-byte copies of the general kernel)
+  // rows staged by one bulk copy each, or by 16-byte copies spread over the lanes (row_copy 1)
   p.lean = false;
-  if (!plain && !with_old && p.gather == 0 && p.hash_log2 == 0 && p.ctx == 1 && cfg.row_copy != 1 &&
-      lean_supported(d)) {
+  if (!plain && !with_old && p.gather == 0 && p.hash_log2 == 0 && p.ctx == 1 && lean_supported(d)) {
     const int nbpad = std::max(32, ((std::max(d.maxM, d.maxM0) + 31) / 32) * 32);
+    const bool bulk = cfg.row_copy != 1;
     int rows = p.stage_rows;
-    cap_bulk_round(d, &rows);  // the lean kernel stages every row by bulk copy
+    if (bulk) cap_bulk_round(d, &rows);
     const int ws = lean_smem_bytes(d, p.region, nbpad, rows);
     if (ws <= kMaxSmemPerBlock) {
       p.lean = true;
+      p.bulk_rows = bulk;
       p.nbpad = nbpad;
       p.stage_rows = rows;
       p.warp_smem = ws;

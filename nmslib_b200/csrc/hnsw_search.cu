@@ -287,23 +287,6 @@ __device__ void compute_dists(const DevIndex& ix, const float* __restrict__ q, c
   }
 }
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-
-// waits until at most N of this thread's committed copy groups are still in flight
-template <int N>
-__device__ __forceinline__ void cp_async_wait_keep() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
-
 // Distances to rows ids[0..n) through the warp's staging area: each round copies up to
 // `stage_rows` rows into shared memory with asynchronous 16-byte copies (every row of the round
 // in flight at once, no registers held), then the four 8-lane groups reduce them.

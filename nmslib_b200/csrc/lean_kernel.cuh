@@ -102,13 +102,15 @@ struct LeanWarp {  // a warp's shared-memory pieces and counters
   uint8_t* vis;
   uint32_t phase;
   int stage_rows;
+  bool bulk;  // rows by one bulk copy each (else 16-byte asynchronous copies spread over the lanes)
   int st_dist, st_expand, st_greedy, st_list_ints;
 };
 
 // Distances to the rows the lanes hold (lane l: up to NCH rows, has[h] / position pos[h] in the
 // step's row list / vector id[h]) into w.nb_d[pos]. Rows go through the staging area in rounds of
-// stage_rows, each row one bulk copy issued by the lane that holds it, completing on the warp's
-// mbarrier. Returns false if the copies did not complete within the wait bound.
+// stage_rows: with w.bulk each row is one bulk copy issued by the lane that holds it, completing on
+// the warp's mbarrier; otherwise the round's ids are posted in w.sv and every lane copies 16-byte
+// pieces of the round's rows. Returns false if bulk copies did not complete within the wait bound.
 template <int NF, bool HALF, int SP, int NCH>
 __device__ bool lean_rows(const DevIndex& ix, LeanWarp& w, const LeanQuery<NF, HALF>& q, const bool (&has)[NCH],
                           const int (&pos)[NCH], const int (&id)[NCH], int nrows) {
@@ -117,21 +119,35 @@ __device__ bool lean_rows(const DevIndex& ix, LeanWarp& w, const LeanQuery<NF, H
   const int lane = lane_id(), g = lane >> 3;
   for (int base = 0; base < nrows; base += w.stage_rows) {
     const int rows = min(w.stage_rows, nrows - base);
-    if (lane == 0) sm100::mbar_arrive_expect_tx(w.bar, (uint32_t)rows * kRowBytes);
-    __syncwarp();
+    if (w.bulk) {
+      if (lane == 0) sm100::mbar_arrive_expect_tx(w.bar, (uint32_t)rows * kRowBytes);
+      __syncwarp();
 #pragma unroll
-    for (int h = 0; h < NCH; ++h) {
-      if (has[h] && pos[h] >= base && pos[h] < base + rows) {
-        sm100::fence_proxy_async_smem();
-        sm100::bulk_copy_g2s(w.stage + (pos[h] - base) * kDim, ix.vecs + (int64_t)id[h] * ix.pitch, kRowBytes,
-                             w.bar);
+      for (int h = 0; h < NCH; ++h) {
+        if (has[h] && pos[h] >= base && pos[h] < base + rows) {
+          sm100::fence_proxy_async_smem();
+          sm100::bulk_copy_g2s(w.stage + (pos[h] - base) * kDim, ix.vecs + (int64_t)id[h] * ix.pitch, kRowBytes,
+                               w.bar);
+        }
       }
-    }
-    const bool ok = sm100::mbar_wait(w.bar, w.phase);
-    w.phase ^= 1;
-    if (!ok) {
-      sm100::mbar_wait(w.bar, w.phase ^ 1);  // bounded: no copy may be left writing the staging rows
-      return false;
+      const bool ok = sm100::mbar_wait(w.bar, w.phase);
+      w.phase ^= 1;
+      if (!ok) {
+        sm100::mbar_wait(w.bar, w.phase ^ 1);  // bounded: no copy may be left writing the staging rows
+        return false;
+      }
+    } else {
+      constexpr int kPieces = kRowBytes / 16;  // 16-byte pieces per row
+#pragma unroll
+      for (int h = 0; h < NCH; ++h)
+        if (has[h] && pos[h] >= base && pos[h] < base + rows) w.sv[pos[h] - base] = id[h];
+      __syncwarp();
+      for (int c = lane; c < rows * kPieces; c += 32) {
+        const int r = c / kPieces, p = c - r * kPieces;
+        cp_async16(w.stage + r * kDim + 4 * p, ix.vecs + (int64_t)w.sv[r] * ix.pitch + 4 * p);
+      }
+      cp_async_wait_all();
+      __syncwarp();
     }
     for (int r0 = 0; r0 < rows; r0 += 4) {
       const int r = r0 + g;
@@ -141,6 +157,47 @@ __device__ bool lean_rows(const DevIndex& ix, LeanWarp& w, const LeanQuery<NF, H
     }
     __syncwarp();
   }
+  return true;
+}
+
+// One expansion's kept neighbours merged into items[0..num) (num <= cap <= 64) through registers:
+// lane t holds list-order neighbour t (key d, id idt, kept or not), lane l array items l and l+32.
+// Each array item moves right by the number of kept keys below it; each kept item lands at (array
+// keys below it) + (kept keys below it). When no kept key equals another kept key or an array key,
+// that is the array that sorting the batch and inserting its items one by one with
+// push_or_replace_non_empty_exp (sort_arr_bi.h:159-199) leaves, truncated to cap, and the smallest
+// insertion index is the kept minimum's. With such a tie it returns false and changes nothing.
+__device__ __forceinline__ bool lean_merge64(uint2* items, int& num, int cap, float d, int idt, bool keep,
+                                             int* first_pos) {
+  const int lane = lane_id();
+  const unsigned km = __ballot_sync(kFull, keep);
+  const bool h0 = lane < num, h1 = lane + 32 < num;
+  const uint2 it0 = h0 ? items[lane] : make_uint2(0u, 0u);
+  const uint2 it1 = h1 ? items[lane + 32] : make_uint2(0u, 0u);
+  const float k0 = key_of(it0), k1 = key_of(it1);
+  int rank = 0, lb = 0, c0 = 0, c1 = 0;
+  bool tie = false;
+  for (unsigned mm = km; mm; mm &= mm - 1) {
+    const int u = __ffs(mm) - 1;
+    const float ku = __shfl_sync(kFull, d, u);
+    rank += ku < d;
+    tie |= (keep && u != lane && ku == d) || (h0 && k0 == ku) || (h1 && k1 == ku);
+    const unsigned b0 = __ballot_sync(kFull, h0 && k0 < ku);
+    const unsigned b1 = __ballot_sync(kFull, h1 && k1 < ku);
+    if (lane == u) lb = __popc(b0) + __popc(b1);
+    c0 += ku < k0;
+    c1 += ku < k1;
+  }
+  if (__any_sync(kFull, tie)) return false;
+  const int p = lb + rank;
+  const int first = __shfl_sync(kFull, p, __ffs(__ballot_sync(kFull, keep && rank == 0)) - 1);
+  __syncwarp();
+  if (h0 && lane + c0 < cap) items[lane + c0] = it0;
+  if (h1 && lane + 32 + c1 < cap) items[lane + 32 + c1] = it1;
+  if (keep && p < cap) items[p] = make_item(d, idt, false);
+  num = min(num + __popc(km), cap);
+  *first_pos = first;
+  __syncwarp();
   return true;
 }
 
@@ -297,10 +354,24 @@ __device__ bool lean_query(const SearchArgs& a, LeanWarp& w, int64_t qi, uint8_t
     w.st_list_ints += 1 + cnt;
     w.st_dist += nnew;
     if (!lean_rows<NF, HALF, SP, NCH>(ix, w, q, has, pos, id, nnew)) return false;
-    // keep d < topKey || size < ef, preserving list order
+    // keep d < topKey || size < ef (lists of up to 32 and arrays of up to 64: merged in registers
+    // unless keys tie)
+    bool merged = false;
+    if constexpr (NCH == 1) {
+      if (cap <= 64) {
+        const bool valid = lane < nnew;
+        const float d = valid ? w.nb_d[lane] : 0.0f;
+        const int idt = valid ? w.nb_id[lane] : 0;
+        const bool keep = valid && ((d < top_key) || (size_now < ef));
+        int p0 = 0x7fffffff;
+        merged = !__any_sync(kFull, keep) || lean_merge64(w.items, num, cap, d, idt, keep, &p0);
+        if (p0 < curr) curr = p0;
+      }
+    }
+    // otherwise: the kept ones in list order, then the batch merge or sort + insertion
     int qty = 0;
 #pragma unroll
-    for (int h = 0; h < NCH; ++h) {
+    for (int h = 0; h < NCH && !merged; ++h) {
       const int t = 32 * h + lane;
       bool keep = false;
       float d = 0.0f;
@@ -319,7 +390,7 @@ __device__ bool lean_query(const SearchArgs& a, LeanWarp& w, int64_t qi, uint8_t
       qty += __popc(mk);
     }
     __syncwarp();
-    if (qty) {
+    if (qty && !merged) {
       int p0;
       if (merge_unsorted_batch(w.items, num, cap, w.sk, w.sv, qty, w.nb_d, w.nb_id, &p0)) {
         if (p0 < curr) curr = p0;
@@ -375,6 +446,7 @@ __global__ void __launch_bounds__(128, 8) search_lean_kernel(SearchArgs a) {
   w.vis = a.visited + (int64_t)slot * a.visited_pitch;
   w.phase = 0;
   w.stage_rows = a.stage_rows;
+  w.bulk = a.bulk_rows != 0;
   if (lane == 0) {
     sm100::mbar_init(w.bar, 1);
     sm100::fence_barrier_init();

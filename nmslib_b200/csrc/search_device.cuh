@@ -30,6 +30,24 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// asynchronous 16-byte global -> shared copies (cp.async, L2 only)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// waits until at most N of this thread's committed copy groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait_keep() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // ------------------------------------------------------------------ libstdc++ sort order
 // Restatement of the algorithm libstdc++ uses for std::sort on random-access ranges
 // (introsort with median-of-three pivot into the first slot, unguarded partition, a 16-element
