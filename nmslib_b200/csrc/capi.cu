@@ -66,14 +66,21 @@ int upload_index(nmsg_index* h) {
   std::vector<float> vec((size_t)n * d.pitch, 0.0f);
   std::vector<int32_t> l0((size_t)n * d.l0_pitch, 0);
   std::vector<int32_t> ext(n);
+  std::vector<uint32_t> seen_in(n, 0);  // 1 + the last node whose list held each id
+  bool unique = true;
   for (int64_t i = 0; i < n; ++i) {
     const float* src = hi.vec(i);
     float* dst = vec.data() + i * d.pitch;
     for (int e = 0; e < hi.dim; ++e) dst[permuted_pos(e, hi.dim)] = src[e];
     const int32_t* lst = hi.l0(i);
     std::memcpy(l0.data() + i * d.l0_pitch, lst, 4 * (1 + lst[0]));
+    for (int t = 1; t <= lst[0]; ++t) {  // ids were validated (< n) when the file was read
+      if (seen_in[lst[t]] == (uint32_t)(i + 1)) unique = false;
+      seen_in[lst[t]] = (uint32_t)(i + 1);
+    }
     ext[i] = hi.ext_id(i);
   }
+  d.l0_unique = unique ? 1 : 0;
   std::vector<int32_t> links = hi.up_links;
   if (links.empty()) links.push_back(0);
   NMSG_CUDA(h->vecs.ensure(vec.size() * 4, false), "cudaMalloc(vectors)");

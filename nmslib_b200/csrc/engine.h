@@ -99,6 +99,8 @@ struct DevIndex {
   int n16 = 0, n4 = 0;
   int maxM = 0, maxM0 = 0, maxlevel = 0, enterpoint = 0, dist_type = 0;
   int row_bytes = 0;                // algorithmic bytes of one row: 4 dim, or 132 for l2sqr_sift
+  int l0_unique = 0;                // 1: no level-0 list repeats an id (checked at upload), so a
+                                    // list's visited checks need no duplicate vote
 };
 
 // Position of element e of a vector in the permuted device row.

@@ -65,6 +65,18 @@ __device__ __forceinline__ float lean_combine(float acc) {
   }
 }
 
+// Two single-precision subtractions in one packed instruction (sub.rn.f32x2): each half is the
+// IEEE-754 binary32 difference rounded to nearest even, the same value as __fsub_rn on that half.
+__device__ __forceinline__ float2 sub2_rn(float2 a, float2 b) {
+  unsigned long long ra, rb, rd;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(ra) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(rb) : "f"(b.x), "f"(b.y));
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+  float2 d;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(rd));
+  return d;
+}
+
 template <int NF, bool HALF>
 struct LeanQuery {
   float4 c[NF > 0 ? NF : 1];
@@ -78,15 +90,30 @@ __device__ __forceinline__ float lean_row_dist(const LeanQuery<NF, HALF>& q, con
 #pragma unroll
   for (int c = 0; c < NF; ++c) {
     const float4 x = reinterpret_cast<const float4*>(row + c * 32)[j];
-    acc = lean_term<SP>(q.c[c].x, x.x, acc);
-    acc = lean_term<SP>(q.c[c].y, x.y, acc);
-    acc = lean_term<SP>(q.c[c].z, x.z, acc);
-    acc = lean_term<SP>(q.c[c].w, x.w, acc);
+    if constexpr (SP == 0) {  // the differences two at a time, the sum of squares in order
+      const float2 d01 = sub2_rn(make_float2(q.c[c].x, q.c[c].y), make_float2(x.x, x.y));
+      const float2 d23 = sub2_rn(make_float2(q.c[c].z, q.c[c].w), make_float2(x.z, x.w));
+      acc = __fmaf_rn(d01.x, d01.x, acc);
+      acc = __fmaf_rn(d01.y, d01.y, acc);
+      acc = __fmaf_rn(d23.x, d23.x, acc);
+      acc = __fmaf_rn(d23.y, d23.y, acc);
+    } else {
+      acc = lean_term<SP>(q.c[c].x, x.x, acc);
+      acc = lean_term<SP>(q.c[c].y, x.y, acc);
+      acc = lean_term<SP>(q.c[c].z, x.z, acc);
+      acc = lean_term<SP>(q.c[c].w, x.w, acc);
+    }
   }
   if constexpr (HALF) {
     const float2 x = reinterpret_cast<const float2*>(row + NF * 32)[j];
-    acc = lean_term<SP>(q.h.x, x.x, acc);
-    acc = lean_term<SP>(q.h.y, x.y, acc);
+    if constexpr (SP == 0) {
+      const float2 d = sub2_rn(q.h, x);
+      acc = __fmaf_rn(d.x, d.x, acc);
+      acc = __fmaf_rn(d.y, d.y, acc);
+    } else {
+      acc = lean_term<SP>(q.h.x, x.x, acc);
+      acc = lean_term<SP>(q.h.y, x.y, acc);
+    }
   }
   return lean_combine<SP>(acc);
 }
@@ -335,8 +362,11 @@ __device__ bool lean_query(const SearchArgs& a, LeanWarp& w, int64_t qi, uint8_t
 #pragma unroll
     for (int h = 0; h < NCH; ++h) {
       const bool valid = 32 * h + lane < cnt;
-      const unsigned same = __match_any_sync(kFull, valid ? idv[h] : -1 - lane);
-      const bool cand = valid && (__ffs(same) - 1) == lane;
+      bool cand = valid;
+      if (!ix.l0_unique) {  // the first of equal ids in the chunk is checked, as a serial walk would
+        const unsigned same = __match_any_sync(kFull, valid ? idv[h] : -1 - lane);
+        cand = valid && (__ffs(same) - 1) == lane;
+      }
       bool isnew = false;
       if (cand) {
         isnew = w.vis[idv[h]] != epoch;

@@ -3,6 +3,7 @@ recorded outputs, on every committed fixture. Distances must be bit-identical; i
 the oracle (both order equal distances by node index) and identical to the reference except
 inside runs of equal distance (the reference orders those by object address)."""
 import os
+import struct
 
 import numpy as np
 import pytest
@@ -318,3 +319,37 @@ def test_bulk_row_copies_in_the_general_kernel(name, si, stage):
             np.testing.assert_array_equal(st, ost)
     finally:
         idx.setLaunchConfig()
+
+
+def test_lists_that_repeat_an_id(tmp_path):
+    """Level-0 lists that name one neighbour twice (the reference visits it once: the second
+    occurrence finds it visited). Such a file turns off the lean kernel's duplicate-free fast path;
+    ids, distances and per-query counts stay the oracle's. The unmodified fixture, whose lists are
+    duplicate-free, takes the fast path in every other test."""
+    name = "c1_l2_d128"
+    raw = bytearray(open(golden_path(name), "rb").read())
+    n, mem, off0 = struct.unpack_from("<IQQ", raw, 4)
+    header = 68  # flag, n, mem_per_obj, off_level0, off_data, maxlevel, enterpoint, maxM, maxM0, dist, method
+    changed = 0
+    for i in range(0, n, 3):
+        p = header + i * mem + off0
+        cnt = struct.unpack_from("<i", raw, p)[0]
+        if cnt >= 3:
+            struct.pack_into("<i", raw, p + 12, struct.unpack_from("<i", raw, p + 4)[0])  # ids[2] = ids[0]
+            changed += 1
+    assert changed > 100
+    path = tmp_path / "repeated_ids.hnsw"
+    path.write_bytes(bytes(raw))
+    idx = nmslib.init(method="hnsw", space="l2")
+    idx.loadIndex(str(path))
+    orc = OracleIndex(str(path))
+    q = load_golden(name)["queries"]
+    for ef in (10, 64, 300):
+        idx.setQueryTimeParams({"efSearch": ef, "algoType": "v1merge"})
+        oi, od, oc, ost = orc.search(q, k=10, ef=ef, algo=ALGO_CODES["v1merge"])
+        for plain in (False, True):
+            ids, d, cnt, st = idx.knnQueryBatchArrays(q, 10, plain=plain, stats=True)
+            np.testing.assert_array_equal(cnt, oc)
+            np.testing.assert_array_equal(ids, oi)
+            np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
+            np.testing.assert_array_equal(st, ost)
