@@ -49,9 +49,16 @@ constexpr int KB_MAX = 4;               // padded dim <= 256 with the query bloc
 constexpr int KB_STREAM_MAX = 64;       // padded dim <= 4096 with query K-blocks streamed per stage
 constexpr int Q_BLOCK_BYTES = BM * BK * 2;   // 16 KB
 constexpr int X_STAGE_BYTES = BN * BK * 2;   // 32 KB
-constexpr int EPI_WARPS = 8;            // two warps per TMEM lane quarter, one per column half
+constexpr int EPI_WARPS = 8;            // sample pass: two warps per TMEM lane quarter, one per column half
 constexpr int HALVES = 2;
-constexpr int kThreads = (EPI_WARPS + 2) * 32;  // + TMA warp + MMA warp
+constexpr int SCAN_EPI_WARPS = 16;      // full scan: four warps per lane quarter, one per column quarter
+constexpr int SCAN_PARTS = 4;
+// Warps of each pass: its epilogue warps, then the TMA warp and the MMA warp.
+template <int MODE>
+struct Roles {
+  static constexpr int kEpi = MODE == 1 ? SCAN_EPI_WARPS : EPI_WARPS;
+  static constexpr int kThreads = (kEpi + 2) * 32;
+};
 constexpr int LIST_STRIDE = CAND + 1;   // +1: rows of a list on different banks
 constexpr int kCollectLen = 64;         // entries of a full-scan list (query, chunk, column half)
 
@@ -70,13 +77,14 @@ struct GemmArgs {
   int per_column;     // sample pass: offer every column, not only each 32-column group's best
   int key_l2;         // 1: key = 2 dot - |x|^2, 0: key = dot
   const float* xnorm2;  // |x|^2 (l2) or 0, +inf for the padding rows up to n_tiles * BN
-  // one list of list_len entries per (query, chunk, column half), written only by the thread
-  // that owns that query row in that work item: mode 0 the best group maxima (list_len = CAND),
-  // mode 1 the rows whose key reaches tau (the count may exceed list_len: the list overflowed)
+  // one list of list_len entries per (query, chunk, column part), written only by the thread
+  // that owns that query row in that work item: mode 0 the best group maxima of a column half
+  // (list_len = CAND), mode 1 the rows of a column quarter whose key reaches tau (the count may
+  // exceed list_len: the list overflowed)
   int list_len;
-  float* list_key;    // [nq][n_chunks * HALVES][list_len]
+  float* list_key;    // [nq][n_chunks * parts][list_len], parts = HALVES (mode 0) or SCAN_PARTS (1)
   int32_t* list_id;
-  int32_t* list_cnt;  // [nq][n_chunks * HALVES]
+  int32_t* list_cnt;  // [nq][n_chunks * parts]
   const float* tau;   // [nq]
   const uint8_t* q_active;  // [q_blocks * BM]
   int32_t* status;
@@ -115,13 +123,11 @@ __device__ __forceinline__ int next_active_item(const GemmArgs& a, int item, int
   return item;
 }
 
-// v[i] for a lane-dependent i, by five levels of selects (no local memory).
-__device__ __forceinline__ float pick32(const float (&v)[32], int i) {
-  float a[16];
+// v[i] of 16 values for a lane-dependent i, by four levels of selects.
+__device__ __forceinline__ float pick16(const float (&v)[16], int i) {
+  float a[8];
 #pragma unroll
-  for (int t = 0; t < 16; ++t) a[t] = (i & 16) ? v[t + 16] : v[t];
-#pragma unroll
-  for (int t = 0; t < 8; ++t) a[t] = (i & 8) ? a[t + 8] : a[t];
+  for (int t = 0; t < 8; ++t) a[t] = (i & 8) ? v[t + 8] : v[t];
 #pragma unroll
   for (int t = 0; t < 4; ++t) a[t] = (i & 4) ? a[t + 4] : a[t];
 #pragma unroll
@@ -168,7 +174,7 @@ __device__ __forceinline__ void list_offer(float* lk, int32_t* li, int& nfill, f
 // MODE 0: the sample pass (per-row candidate heaps); MODE 1: the full scan (threshold lists).
 // Compiled separately so that each carries only its own epilogue code.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(Roles<MODE>::kThreads, 1)
     bf16_scan_kernel(const __grid_constant__ CUtensorMap tmq, const __grid_constant__ CUtensorMap tmx, GemmArgs a) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -201,7 +207,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(q_empty, 1);
     for (int i = 0; i < 2; ++i) {
       mbar_init(&acc_full[i], 1);
-      mbar_init(&acc_empty[i], EPI_WARPS);  // one arrival per epilogue warp
+      mbar_init(&acc_empty[i], Roles<MODE>::kEpi);  // one arrival per epilogue warp
     }
     mbar_init(mma_drain, 1);
     fence_barrier_init();
@@ -212,7 +218,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
 
-  if (warp == EPI_WARPS) {
+  if (warp == Roles<MODE>::kEpi) {
     // ------------------------------------------------ TMA producer
     // A load is issued only after its slot's empty barrier completed. After a failed wait nothing
     // more is issued, and before the role ends it waits (bounded) for the last load armed on each
@@ -266,7 +272,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       if (q_armed > 0 && !mbar_wait(q_full, (uint32_t)((q_armed - 1) & 1))) ok = false;
     }
-  } else if (warp == EPI_WARPS + 1) {
+  } else if (warp == Roles<MODE>::kEpi + 1) {
     // ------------------------------------------------ MMA issuer
     // No MMA and no commit is issued after a failed wait. Every MMA reads operands whose full
     // barrier completed, and before the role ends one last commit (only if an MMA was ever issued)
@@ -326,9 +332,108 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!mbar_wait(mma_drain, 0)) ok = false;
       }
     }
+  } else if constexpr (MODE == 1) {
+    // ------------------------------------------------ epilogue of the full scan: warps 0-15. Warp w
+    // reads TMEM lane quarter w & 3 (thread = one query row) and the 64 columns of part w >> 2 of
+    // each tile, 16 at a time: four warps per scheduler hide the latency of the threshold test and
+    // of the rare hit path, which two warps per scheduler left exposed.
+    constexpr int CW = BN / SCAN_PARTS;  // columns per warp
+    const int quarter = warp & 3, part = warp >> 2;
+    const int row = quarter * 32 + lane;
+    float* snw = snrm + warp * CW;  // |x|^2 of this warp's columns of the tile
+    uint32_t accphase[2] = {0, 0};
+    int tcount = 0;
+    for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
+      const int qb = item % a.q_blocks, chunk = item / a.q_blocks;
+      if (!item_active<MODE>(a, qb)) continue;
+      const int q = qb * BM + row;
+      const bool qvalid = q < a.nq;
+      // tau, with a finite floor so the -inf keys of columns past the last row never qualify
+      const float thr = (qvalid && a.q_active[q]) ? fmaxf(a.tau[q], -FLT_MAX) : INFINITY;
+      const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
+      // |x|^2 of this part's columns, 4 per lane in lanes 0-15, loaded one tile ahead
+      const float4* xn4 = reinterpret_cast<const float4*>(a.xnorm2) + part * (CW / 4) + (lane & 15);
+      float4 nrm_next = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (t0 < t1) nrm_next = __ldg(xn4 + (size_t)t0 * a.tile_step * (BN / 4));
+      const float ks = a.key_l2 ? 2.0f : 1.0f;
+      const size_t list = ((size_t)q * a.n_chunks + chunk) * SCAN_PARTS + part;
+      int32_t* cid = a.list_id + list * a.list_len;
+      float* ckey = a.list_key + list * a.list_len;
+      int ncoll = 0;
+      for (int vt = t0; vt < t1 && ok; ++vt, ++tcount) {
+        const int t = vt * a.tile_step;
+        const int buf = tcount & 1;
+        __syncwarp();  // every lane is done with the previous tile's norms
+        if (lane < CW / 4) reinterpret_cast<float4*>(snw)[lane] = nrm_next;
+        if (vt + 1 < t1) nrm_next = __ldg(xn4 + (size_t)(t + a.tile_step) * (BN / 4));
+        __syncwarp();
+        ok = mbar_wait(&acc_full[buf], accphase[buf]);
+        accphase[buf] ^= 1;
+        tc_fence_after();
+        // TMEM loads of the next 16 columns overlap the work on the current ones
+        const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + buf * BN + part * CW;
+        uint32_t ra[16];
+        tmem_ld16_issue(tb, ra);
+        tmem_ld_wait16(ra);
+#pragma unroll 1
+        for (int c = 0; c < CW / 16; ++c) {
+          uint32_t cur[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) cur[i] = ra[i];
+          if (c + 1 < CW / 16) {
+            tmem_ld16_issue(tb + 16 * (c + 1), ra);
+          } else {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[buf]);  // this warp's part of the accumulator is read
+          }
+          const int col0 = t * BN + part * CW + c * 16;
+          // keys: ks * acc - xnorm2, as in the sample pass; rows past the base have key -inf
+          float v[16];
+          const float4* nv = reinterpret_cast<const float4*>(snw + c * 16);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const float4 x4 = nv[j];  // same address in every lane: a broadcast
+            v[4 * j + 0] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 0]), -x4.x);
+            v[4 * j + 1] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 1]), -x4.y);
+            v[4 * j + 2] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 2]), -x4.z);
+            v[4 * j + 3] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 3]), -x4.w);
+          }
+          float m[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) m[i] = fmaxf(v[i], v[i + 8]);
+#pragma unroll
+          for (int w = 4; w > 0; w >>= 1)
+#pragma unroll
+            for (int i = 0; i < w; ++i) m[i] = fmaxf(m[i], m[i + w]);
+          // one warp vote first: the common case (no row of the warp passes) skips the rest
+          if (__any_sync(0xffffffffu, m[0] >= thr)) {
+            // this row's hits as a bit mask built with selects, then one store pair per hit in a
+            // loop whose trip count is the warp's largest hit count, plain stores into the row's list
+            unsigned hm = 0;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) hm |= (v[i] >= thr ? 1u : 0u) << i;
+            while (__any_sync(0xffffffffu, hm != 0)) {
+              if (hm) {
+                const int i = __ffs(hm) - 1;
+                hm &= hm - 1;
+                if (ncoll < a.list_len) {
+                  cid[ncoll] = col0 + i;
+                  ckey[ncoll] = pick16(v, i);
+                }
+                ++ncoll;
+              }
+            }
+          }
+          __syncwarp();
+          if (c + 1 < CW / 16) tmem_ld_wait16(ra);
+        }
+      }
+      if (qvalid) a.list_cnt[list] = ncoll;
+    }
   } else {
-    // ------------------------------------------------ epilogue: warps 0-7; thread = one query row
-    // (TMEM lane) for one half of the tile's columns, 32 columns at a time
+    // ------------------------------------------------ epilogue of the sample pass: warps 0-7; thread
+    // = one query row (TMEM lane) for one half of the tile's columns, 32 columns at a time
     const int quarter = warp & 3, half = warp >> 2;
     const int row = quarter * 32 + lane;
     float* lk = skey + (half * BM + row) * LIST_STRIDE;
@@ -341,10 +446,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!item_active<MODE>(a, qb)) continue;
       const int q = qb * BM + row;
       const bool qvalid = q < a.nq;
-      float thr = -INFINITY;  // mode 0: the list's smallest key once full; mode 1: tau
+      float thr = -INFINITY;  // the list's smallest key once full
       int nfill = 0;
-      // mode 1: a finite floor, so the -inf keys of columns past the last row never qualify
-      if (MODE == 1) thr = (qvalid && a.q_active[q]) ? fmaxf(a.tau[q], -FLT_MAX) : INFINITY;
       const int t0 = chunk * a.chunk_tiles, t1 = min(a.n_tiles, t0 + a.chunk_tiles);
       // |x|^2 of this half's 128 columns, 4 per lane, loaded one tile ahead
       const float4* xn4 = reinterpret_cast<const float4*>(a.xnorm2) + half * (BN / HALVES / 4) + lane;
@@ -354,7 +457,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       const size_t list = ((size_t)q * a.n_chunks + chunk) * HALVES + half;
       int32_t* cid = a.list_id + list * a.list_len;
       float* ckey = a.list_key + list * a.list_len;
-      int ncoll = 0;
       for (int vt = t0; vt < t1 && ok; ++vt, ++tcount) {
         const int t = vt * a.tile_step;
         const int buf = tcount & 1;
@@ -404,63 +506,35 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int i = 0; i < w; ++i) m[i] = fmaxf(m[i], m[i + w]);
           const float mx = m[0];
-          if constexpr (MODE == 0) {
-            if (a.per_column) {
-              // small bases (the sample is all of it): every column is offered
-              if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
-                float vl[32];
+          if (a.per_column) {
+            // small bases (the sample is all of it): every column is offered
+            if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
+              float vl[32];
 #pragma unroll
-                for (int i = 0; i < 32; ++i) vl[i] = v[i];
+              for (int i = 0; i < 32; ++i) vl[i] = v[i];
 #pragma unroll 1
-                for (int i = 0; i < 32; ++i)
-                  if ((vl[i] > thr || nfill < CAND) && vl[i] > -INFINITY)
-                    list_offer(lk, li, nfill, thr, vl[i], col0 + i);
-              }
-            } else if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
-              // the group's best column is the candidate: the lists hold distinct base vectors,
-              // so the exact k-th key among them still bounds the true k-th key from below
-              int arg = 31;
-#pragma unroll
-              for (int i = 30; i >= 0; --i) arg = v[i] == mx ? i : arg;
-              list_offer(lk, li, nfill, thr, mx, col0 + arg);
+              for (int i = 0; i < 32; ++i)
+                if ((vl[i] > thr || nfill < CAND) && vl[i] > -INFINITY)
+                  list_offer(lk, li, nfill, thr, vl[i], col0 + i);
             }
-          } else {
-            // one warp vote first: the common case (no row of the warp passes) skips the
-            // divergent region entirely
-            if (__any_sync(0xffffffffu, mx >= thr)) {
-              // this row's hits as a bit mask built with selects (no branch per column), then one
-              // store pair per hit in a loop whose trip count is the warp's largest hit count
-              // (usually 1), the key taken out of the registers by a select tree: plain stores
-              // into the row's own list
-              unsigned hm = 0;
+          } else if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
+            // the group's best column is the candidate: the lists hold distinct base vectors,
+            // so the exact k-th key among them still bounds the true k-th key from below
+            int arg = 31;
 #pragma unroll
-              for (int i = 0; i < 32; ++i) hm |= (v[i] >= thr ? 1u : 0u) << i;
-              while (__any_sync(0xffffffffu, hm != 0)) {
-                if (hm) {
-                  const int i = __ffs(hm) - 1;
-                  hm &= hm - 1;
-                  if (ncoll < a.list_len) {
-                    cid[ncoll] = col0 + i;
-                    ckey[ncoll] = pick32(v, i);
-                  }
-                  ++ncoll;
-                }
-              }
-            }
+            for (int i = 30; i >= 0; --i) arg = v[i] == mx ? i : arg;
+            list_offer(lk, li, nfill, thr, mx, col0 + arg);
           }
           __syncwarp();
           if (c + 1 < BN / HALVES / 32) tmem_ld_wait(ra);
         }
       }
       if (qvalid) {
-        if (MODE == 0) {
-          for (int j = 0; j < nfill; ++j) {
-            ckey[j] = lk[j];
-            cid[j] = li[j];
-          }
-          ncoll = nfill;
+        for (int j = 0; j < nfill; ++j) {
+          ckey[j] = lk[j];
+          cid[j] = li[j];
         }
-        a.list_cnt[list] = ncoll;
+        a.list_cnt[list] = nfill;
       }
     }
   }
@@ -1052,9 +1126,24 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   // of the base; split into chunks so the sample pass also fills the GPU for small batches
   const int s_tiles = std::min(n_tiles, std::max(16, n_tiles / 16));
   const int s_step = n_tiles / s_tiles;
-  int s_chunks = std::max(1, std::min(s_tiles / 4, h->num_sms / q_blocks));
-  const int s_chunk_tiles = (s_tiles + s_chunks - 1) / s_chunks;
-  s_chunks = (s_tiles + s_chunk_tiles - 1) / s_chunk_tiles;
+  // (chunks of at least 4 tiles; the split with the least of: tiles the busiest CTA visits plus the
+  // rerank's cost of the candidate lists each chunk adds per query, which measured on B200 as about
+  // 14 tile visits per chunk for 10K queries, in proportion to the query count)
+  int s_chunks = 1, s_chunk_tiles = s_tiles;
+  {
+    const double per_chunk = 14.0 * (double)nq / 10000.0;
+    double best = 1e300;
+    for (int c = 1; c <= std::max(1, s_tiles / 4); ++c) {
+      const int ct = (s_tiles + c - 1) / c, cc = (s_tiles + ct - 1) / ct;
+      const int64_t rounds = ((int64_t)q_blocks * cc + h->num_sms - 1) / h->num_sms;
+      const double cost = (double)rounds * ct + per_chunk * cc;
+      if (cost < best - 1e-9) {
+        best = cost;
+        s_chunks = cc;
+        s_chunk_tiles = ct;
+      }
+    }
+  }
   // the full scan: about 8 or more work items per CTA, the split whose busiest CTA carries the
   // least excess over the average (items are dealt round-robin)
   int chunk_tiles = n_tiles, n_chunks = 1;
@@ -1087,7 +1176,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   BF_CUDA(s->qn_hi.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->qn_lo.ensure(nq * 4, false), "cudaMalloc");
   BF_CUDA(s->eps.ensure(nq * 4, false), "cudaMalloc");
-  const size_t s_lists = (size_t)nq * s_chunks * HALVES, c_lists = (size_t)nq * n_chunks * HALVES;
+  const size_t s_lists = (size_t)nq * s_chunks * HALVES, c_lists = (size_t)nq * n_chunks * SCAN_PARTS;
   BF_CUDA(s->cand_key.ensure(s_lists * CAND * 4, false), "cudaMalloc");
   BF_CUDA(s->cand_id.ensure(s_lists * CAND * 4, false), "cudaMalloc");
   BF_CUDA(s->cand_cnt.ensure(s_lists * 4, false), "cudaMalloc");
@@ -1141,7 +1230,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   const int smem = SmemLayout(kb, ga.stages, ga.stream_q).total + 1024;
   BF_CUDA((cudaError_t)allow_max_smem((const void*)bf16_scan_kernel<0>), "smem attribute");
   BF_CUDA((cudaError_t)allow_max_smem((const void*)bf16_scan_kernel<1>), "smem attribute");
-  bf16_scan_kernel<0><<<std::min(q_blocks * s_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, ga);
+  bf16_scan_kernel<0><<<std::min(q_blocks * s_chunks, h->num_sms), Roles<0>::kThreads, smem, st>>>(tmq, s->tmx, ga);
   BF_CUDA(cudaGetLastError(), "brute-force scan (sample)");
 
   RerankArgs ra;
@@ -1183,7 +1272,7 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   gb.list_id = s->coll_id.as<int32_t>();
   gb.list_cnt = s->coll_cnt.as<int32_t>();
   RerankArgs rb = ra;
-  rb.n_lists = n_chunks * HALVES;
+  rb.n_lists = n_chunks * SCAN_PARTS;
   rb.list_len = kCollectLen;
   rb.ids = s->coll_id.as<int32_t>();
   rb.bf_keys = s->coll_key.as<float>();
@@ -1202,7 +1291,8 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   for (int attempt = 0; attempt < kScans; ++attempt) {
     BF_CUDA(cudaMemsetAsync(s->found.p, 0, nq * 4, st), "reset counts");
     BF_CUDA(cudaMemsetAsync(s->needs.p, 0, mpad, st), "reset flags");
-    bf16_scan_kernel<1><<<std::min(q_blocks * n_chunks, h->num_sms), kThreads, smem, st>>>(tmq, s->tmx, gb);
+    bf16_scan_kernel<1><<<std::min(q_blocks * n_chunks, h->num_sms), Roles<1>::kThreads, smem, st>>>(tmq, s->tmx,
+                                                                                                   gb);
     BF_CUDA(cudaGetLastError(), "brute-force scan");
     rb.only = attempt == 0 ? nullptr : s->qact.as<uint8_t>();  // the other queries keep their results
     rerank_kernel<<<rr_blocks, 256, 0, st>>>(rb);
@@ -1253,6 +1343,6 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   if (overflow)
     return bf_fail(NMSG_ERR_CAPACITY, std::to_string(overflow) + " queries had more vectors within the BF16 error "
                                       "bound of their k-th neighbour than the scan keeps (" + std::to_string(kCollectLen) +
-                                      " per " + std::to_string(chunk_tiles * BN / HALVES) + " base rows)");
+                                      " per " + std::to_string(chunk_tiles * BN / SCAN_PARTS) + " base rows)");
   return NMSG_OK;
 }

@@ -192,10 +192,12 @@ def test_bruteforce_larger_cosine(tmp_path):
     np.testing.assert_allclose(d, want_d, rtol=2e-6, atol=2e-6)
 
 
-def _far_medium_near(n=40_000, dim=16, seed=5):
+def _far_medium_near(n=40_000, dim=16, seed=5, nq=2560):
     """A base whose sampled tiles hold only far vectors, so the sample's threshold admits every
     other vector: more than the collection holds. Tile t (256 rows) is sampled when t % 9 == 0
-    and t <= 135 (16 of the 157 tiles). Ten near vectors sit in tile 1."""
+    and t <= 135 (16 of the 157 tiles). Ten near vectors sit in tile 1. With 20 blocks of 128
+    queries the full scan's work items span two tiles each, so each 64-entry list of a column
+    quarter sees 128 candidate rows and overflows."""
     rng = np.random.default_rng(seed)
     u = rng.standard_normal((n, dim))
     u /= np.linalg.norm(u, axis=1, keepdims=True)
@@ -203,7 +205,7 @@ def _far_medium_near(n=40_000, dim=16, seed=5):
     sampled = (tile % 9 == 0) & (tile <= 135)
     radius = np.where(sampled, 100.0, 10.0 + 5.0 * rng.random(n))
     radius[256:266] = 1.0 + 0.01 * np.arange(10)
-    return (u * radius[:, None]).astype(np.float32), (0.01 * rng.standard_normal((4, dim))).astype(np.float32)
+    return (u * radius[:, None]).astype(np.float32), (0.01 * rng.standard_normal((nq, dim))).astype(np.float32)
 
 
 def test_bruteforce_rescans_overflowed_queries(tmp_path):
@@ -221,14 +223,16 @@ def test_bruteforce_rescans_overflowed_queries(tmp_path):
 
 
 def test_bruteforce_capacity_error(tmp_path):
-    """17000 identical vectors: every one stays within the error bound of the k-th, twice."""
+    """17000 identical vectors: every one stays within the error bound of the k-th, on every
+    rescan. 4608 queries (36 blocks), so that the full scan's work items span two tiles and its
+    lists can overflow."""
     base = np.tile(np.linspace(-1, 1, 8, dtype=np.float32), (17_000, 1))
     p = str(tmp_path / "same.hnsw")
     _capi.build_index(base, 0, 4, 10, nthreads=0, out_path=p)
     idx = nmslib.init(method="hnsw", space="l2")
     idx.loadIndex(p)
     with pytest.raises(RuntimeError, match="within the BF16 error bound"):
-        idx.bruteForceBatchArrays(base[:2] + 0.5, 10)
+        idx.bruteForceBatchArrays(np.tile(base[:2] + 0.5, (2304, 1)), 10)
 
 
 @pytest.mark.parametrize("k", [1, 10, 32])
