@@ -620,15 +620,21 @@ def aux_workload(which, device=0, serving_rates=(250e3, 500e3, 1e6)):
         k = rng.choice([1, 10, 100], nq).astype(np.int32)
         ef = rng.integers(64, 1025, nq).astype(np.int32)
         dt, (ids, d, cnt) = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
-        # the same launch with the 3840-byte rows staged by 16-byte copies spread over the lanes
-        # instead of one bulk copy per row (the default for rows of 1 KB and more)
-        index.setLaunchConfig(row_copy=1)
-        dt16, _ = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
-        index.setLaunchConfig()
+        # the same launch with the 3840-byte rows staged in shared memory, 8 per round, by one bulk
+        # copy (TMA unit) per row or by 16-byte copies spread over the lanes, against the default
+        # (rows gathered into registers, one per 8-lane group)
+        row_copy = {"register_rows_ms": round(dt * 1e3, 2)}
+        for label, cfg in (("staged_bulk_ms", dict(stage_rows=8, row_copy=2)),
+                           ("staged_cp16_ms", dict(stage_rows=8, row_copy=1))):
+            index.setLaunchConfig(**cfg)
+            dts, (ids_s, _, _) = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
+            index.setLaunchConfig()
+            assert np.array_equal(ids_s, ids), f"{label}: results differ from the default launch"
+            row_copy[label] = round(dts * 1e3, 2)
         truth10 = fp64_truth(base, queries, 10, space)
         sel = k == 10
         out["mixed_batch"] = {"queries": nq, "qps_e2e": round(nq / dt), "ms": round(dt * 1e3, 2),
-                              "row_copy": {"bulk_ms": round(dt * 1e3, 2), "cp16_ms": round(dt16 * 1e3, 2)},
+                              "row_copy": row_copy,
                               "searchold_queries": int((ef >= 1000).sum()),
                               "recall@10_of_k10_queries": round(
                                   recall_at_k(d[sel][:, :10].astype(np.float64), cnt[sel], truth10[sel], 10), 4)}

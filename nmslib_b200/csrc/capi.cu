@@ -175,10 +175,11 @@ int space_matches(int space, int dist_type) {
 namespace nmsg {
 
 // Rows per staging round when every row is one bulk copy completing on the warp's mbarrier: at most
-// kBulkRoundBytes per round (one mbarrier phase). Measured on B200: rounds of 30,720 bytes (8 rows
-// of 960 floats) complete; rounds of 122,880 and 153,600 bytes ran out of the wait bound and the
-// kernel reported NMSG_ERR_TIMEOUT, with the device still answering. The cause is not established,
-// so larger rounds are not issued. Returns whether *rows changed.
+// kBulkRoundBytes per round (one mbarrier phase). On B200, rounds of 122,880 and 153,600 bytes ran
+// out of the wait bound (NMSG_ERR_TIMEOUT, the device still answering) while the general kernels
+// re-initialised the mbarrier at every query of a warp; they now initialise it once per warp, and
+// with that, 8-row rounds of 3,840-byte rows complete at full scale. Larger rounds have not been
+// run since, so they are still not issued. Returns whether *rows changed.
 static bool cap_bulk_round(const DevIndex& d, int* rows) {
   const int cap = std::max(1, kBulkRoundBytes / bulk_row_bytes(d));
   if (*rows <= cap) return false;
@@ -208,6 +209,13 @@ int plan_launch(const DevIndex& d, const nmsg_launch_config& cfg, int region, bo
   } else if (cfg.stage_rows == 0 && cfg.rows_per_group == 0 && d.pitch <= 256) {
     p.gather = 0;
     p.stage_rows = p.region <= 160 ? 8 : 4;
+  } else if (cfg.stage_rows == 0 && cfg.rows_per_group == 0) {
+    // wider rows: staged too, by one bulk copy per row unless 16-byte copies are asked for (rounds
+    // capped below). Measured on B200 for the 1M x 960 negdot mixed batch (8000 queries, per-query
+    // k and efSearch up to 1024): 41.95 ms staged by bulk copies, 47.91 ms staged by 16-byte copies,
+    // 56.04 ms with the rows gathered into registers.
+    p.gather = 0;
+    p.stage_rows = 8;
   } else {
     p.gather = cfg.rows_per_group ? cfg.rows_per_group : (d.pitch <= 256 ? 2 : 1);
   }
@@ -436,12 +444,13 @@ int nmsg_last_device_status(const nmsg_index* h) { return h ? h->last_status : N
 
 int nmsg_set_launch_config(nmsg_index* h, const nmsg_launch_config* cfg) {
   if (!h) return fail(NMSG_ERR_BAD_ARG, "null index");
-  nmsg_launch_config c{0, 0, 0, 0, 0, 0, 0};
+  nmsg_launch_config c{0, 0, 0, 0, 0, 0, 0, 0};
   if (cfg) {
     c = *cfg;
     if (c.plain_slots < 0) return fail(NMSG_ERR_BAD_ARG, "plain_slots must be >= 0");
     if (c.queries_per_warp < 0 || c.queries_per_warp > 4) return fail(NMSG_ERR_BAD_ARG, "queries_per_warp must be 0..4");
     if (c.row_copy < 0 || c.row_copy > 2) return fail(NMSG_ERR_BAD_ARG, "row_copy must be 0, 1 or 2");
+    if (c.query_order != 0 && c.query_order != -1) return fail(NMSG_ERR_BAD_ARG, "query_order must be 0 or -1");
     const int w = c.warps_per_block, r = c.rows_per_group, hl = c.visited_hash_log2, sr = c.stage_rows;
     if (!(w == 0 || w == 1 || w == 2 || w == 4)) return fail(NMSG_ERR_BAD_ARG, "warps_per_block must be 0, 1, 2 or 4");
     if (!(r == 0 || r == 1 || r == 2 || r == 4)) return fail(NMSG_ERR_BAD_ARG, "rows_per_group must be 0, 1, 2 or 4");
@@ -615,6 +624,18 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
     }
   }
   a.nbpad = plan.nbpad;
+  // Split lean search: worth it once the batch outnumbers the resident warps (some warps then run
+  // several queries, and which queries start last decides when the batch ends).
+  if (plan.lean && !plain && !a.order && nq > slots && h->cfg.query_order != -1) {
+    const size_t words = (size_t)nq * 6 + 4;  // node, distance, 3 counts, order; range
+    NMSG_CUDA(h->entry.ensure(words * 4, false), "cudaMalloc(level-0 entries)");
+    int32_t* e = h->entry.as<int32_t>();
+    a.entry_node = e;
+    a.entry_dist = reinterpret_cast<float*>(e + nq);
+    a.entry_stats = e + 2 * nq;
+    a.entry_order = e + 5 * nq;
+    a.entry_range = reinterpret_cast<uint32_t*>(e + 6 * nq);
+  }
   if (dev_ptrs && (flags & NMSG_CUDA_GRAPH)) {
     // Replay the captured launch when every argument is the same as last time; otherwise
     // capture (counter and status resets + kernel) into a new graph.

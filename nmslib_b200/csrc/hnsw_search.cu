@@ -784,8 +784,13 @@ __device__ bool search_old(const SearchArgs& a, WarpCtx& w, int64_t qi, int k, i
   return !overflow;
 }
 
+// bar_phase: the warp's bulk-copy mbarrier phase, kept across its queries; kBarUninit before the
+// warp's first query, which initialises the mbarrier (once per warp: it is never re-initialised
+// while the warp runs).
+constexpr uint32_t kBarUninit = 2;
+
 template <int R, bool OLD>
-__device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi) {
+__device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi, uint32_t& bar_phase) {
   const DevIndex& ix = a.ix;
   const int lane = lane_id();
   WarpCtx w;
@@ -818,11 +823,15 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
   w.failed = false;
   if (a.bulk_rows && a.stage_rows > 0) {
     w.bar = reinterpret_cast<uint64_t*>(w.stage + (size_t)a.stage_rows * ix.pitch);
-    if (lane == 0) {
-      sm100::mbar_init(w.bar, 1);  // idle between queries: every copy was waited for
-      sm100::fence_barrier_init();
+    if (bar_phase == kBarUninit) {
+      if (lane == 0) {
+        sm100::mbar_init(w.bar, 1);
+        sm100::fence_barrier_init();
+      }
+      __syncwarp();
+      bar_phase = 0;
     }
-    __syncwarp();
+    w.phase = bar_phase;
   }
 
   // next epoch of this slot's visited array; clear it when the byte wraps (hnsw.h:582-589)
@@ -851,6 +860,7 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
   } else {
     search_v1merge<R>(a, w, qi, k, ef, cur, curdist);
   }
+  bar_phase = w.phase;
   if (w.failed && lane == 0) {  // a row copy gave up: the query's results are not trusted
     set_status(a.status, NMSG_ERR_TIMEOUT);
     a.counts[qi] = 0;
@@ -873,13 +883,14 @@ __global__ void __launch_bounds__(128, 8) search_batched_kernel(SearchArgs a) {
   char* wsmem = smem + warp * a.warp_smem;
   const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
   if (slot >= a.num_slots) return;
+  uint32_t bar_phase = kBarUninit;
   while (true) {
     int item = 0;
     if (lane == 0) item = atomicAdd(a.work_counter, 1);
     item = __shfl_sync(kFull, item, 0);
     if (item >= a.nq) break;
     const int64_t qi = a.order ? a.order[item] : item;
-    run_query<R, OLD>(a, wsmem, slot, qi);
+    run_query<R, OLD>(a, wsmem, slot, qi, bar_phase);
   }
 }
 
@@ -906,7 +917,8 @@ __global__ void __launch_bounds__(32, 32) search_plain_kernel(SearchArgs a) {
     }
     return;
   }
-  run_query<R, OLD>(a, smem, slot, qi);
+  uint32_t bar_phase = kBarUninit;
+  run_query<R, OLD>(a, smem, slot, qi, bar_phase);
   __threadfence();
   if (lane == 0) atomicExch(a.slot_locks + slot, 0);
 }
@@ -1984,6 +1996,55 @@ int allow_max_smem(const void* kern) {
   return 0;
 }
 
+namespace {
+
+// The level-0 pass's work order: queries by their level-0 entry distance, largest first (the
+// queries that enter level 0 far from their query tend to need the most expansions, and starting
+// them first keeps the batch's end from waiting on a long query that started late). One block:
+// kOrderBuckets buckets spread evenly over the range of the ordered keys, counted, scanned, and
+// filled (the order inside a bucket is arbitrary; results do not depend on the order).
+constexpr int kOrderBuckets = 2048;
+
+__device__ __forceinline__ int order_bucket(float v, uint32_t lo, uint32_t hi) {
+  const uint32_t k = min(max(ordered_key(v), lo), hi);
+  const uint64_t span = hi > lo ? (uint64_t)(hi - lo) : 1;
+  return kOrderBuckets - 1 - (int)(((uint64_t)(k - lo) * (kOrderBuckets - 1)) / span);
+}
+
+__global__ void __launch_bounds__(1024) order_by_entry_kernel(const float* __restrict__ key, int64_t nq,
+                                                             const uint32_t* __restrict__ range,
+                                                             int32_t* __restrict__ order) {
+  __shared__ int cnt[kOrderBuckets];
+  for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) cnt[b] = 0;
+  __syncthreads();
+  const uint32_t lo = range[0], hi = range[1];
+  for (int64_t i = threadIdx.x; i < nq; i += blockDim.x) atomicAdd(&cnt[order_bucket(key[i], lo, hi)], 1);
+  __syncthreads();
+  if (threadIdx.x < 32) {  // exclusive scan: each lane a run of 64 buckets, then across the lanes
+    constexpr int kRun = kOrderBuckets / 32;
+    const int lane = threadIdx.x;
+    int sum = 0;
+    for (int b = 0; b < kRun; ++b) sum += cnt[lane * kRun + b];
+    int pre = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(kFull, pre, o);
+      if (lane >= o) pre += v;
+    }
+    int s = pre - sum;
+    for (int b = 0; b < kRun; ++b) {
+      const int c = cnt[lane * kRun + b];
+      cnt[lane * kRun + b] = s;
+      s += c;
+    }
+  }
+  __syncthreads();
+  for (int64_t i = threadIdx.x; i < nq; i += blockDim.x)
+    order[atomicAdd(&cnt[order_bucket(key[i], lo, hi)], 1)] = (int32_t)i;
+}
+
+}  // namespace
+
 int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, int blocks, int warps_per_block,
                   void* stream) {
   Kern kern = a.lean ? lean_kernel_for(a.ix) : kernel_for(plain, gather, with_old, a.ctx_per_warp, multi_list_chunks(a.ix));
@@ -1991,6 +2052,27 @@ int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, in
   const int smem = a.warp_smem * (plain ? 1 : warps_per_block);
   const int rc = allow_max_smem((const void*)kern);
   if (rc != 0) return rc;
+  if (a.lean && !plain && a.entry_node) {
+    // split: the upper-level descent of every query, the order, then level 0 in that order
+    cudaStream_t st = (cudaStream_t)stream;
+    SearchArgs d = a;
+    d.split = 1;
+    d.order = nullptr;
+    cudaError_t e = cudaMemsetAsync(a.entry_node, 0xff, (size_t)a.nq * 4, st);  // -1: no entry yet
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.entry_dist, 0, (size_t)a.nq * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.entry_range, 0xff, 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.entry_range + 1, 0, 4, st);
+    if (e != cudaSuccess) return (int)e;
+    kern<<<blocks, 32 * warps_per_block, smem, st>>>(d);
+    order_by_entry_kernel<<<1, 1024, 0, st>>>(a.entry_dist, a.nq, a.entry_range, a.entry_order);
+    e = cudaMemsetAsync(a.work_counter, 0, 4, st);
+    if (e != cudaSuccess) return (int)e;
+    SearchArgs l = a;
+    l.split = 2;
+    l.order = a.entry_order;
+    kern<<<blocks, 32 * warps_per_block, smem, st>>>(l);
+    return (int)cudaGetLastError();
+  }
   if (plain)
     kern<<<(unsigned)a.nq, 32, smem, (cudaStream_t)stream>>>(a);
   else

@@ -353,3 +353,82 @@ def test_lists_that_repeat_an_id(tmp_path):
             np.testing.assert_array_equal(ids, oi)
             np.testing.assert_array_equal(d.view(np.int32), od.view(np.int32))
             np.testing.assert_array_equal(st, ost)
+
+
+@pytest.mark.parametrize("row_copy", [2, 1], ids=["bulk", "cp16"])
+def test_staged_wide_rows_many_queries_per_warp(row_copy):
+    """3840-byte rows staged 8 per round through the general kernel for a batch large enough that
+    every warp runs many queries in a row (the row-copy mbarrier is set up once per warp and its
+    phase carried from query to query), SearchOld and V1Merge queries mixed: the oracle's results."""
+    name = "negdot_d960"
+    q = load_golden(name)["queries"]
+    reps = max(1, 24000 // len(q))
+    big = np.ascontiguousarray(np.tile(q, (reps, 1)))
+    rng = np.random.default_rng(11)
+    efs = np.tile(rng.integers(16, 1100, len(q)).astype(np.int32), reps)
+    ks = np.tile(rng.choice([1, 10, 100], len(q)).astype(np.int32), reps)
+    idx = _gpu_index(name)
+    idx.setQueryTimeParams({"efSearch": 20, "algoType": "hybrid"})
+    idx.setLaunchConfig(stage_rows=8, row_copy=row_copy)
+    try:
+        ids, d, cnt, st = idx.knnQueryBatchArrays(big, ks, ef=efs, stats=True)
+    finally:
+        idx.setLaunchConfig()
+    oi, od, oc, ost = _oracle(name).search(q, k=int(ks.max()), ef=20, k_per_q=ks[:len(q)], ef_per_q=efs[:len(q)])
+    np.testing.assert_array_equal(cnt, np.tile(oc, reps))
+    np.testing.assert_array_equal(ids, np.tile(oi, (reps, 1)))
+    np.testing.assert_array_equal(d.view(np.int32), np.tile(od, (reps, 1)).view(np.int32))
+    np.testing.assert_array_equal(st, np.tile(ost, (reps, 1)))
+
+
+@pytest.mark.parametrize("order", [0, -1], ids=["split", "one-pass"])
+@pytest.mark.parametrize("name,si", [("c1_l2_d128", 0), ("c1_l2_d128", 3), ("c1_l2_d128", 6), ("sift_l2_ties", 0),
+                                     ("dup_l2_d16", 2), ("tiny_cos_d48", 0)])
+def test_batches_larger_than_the_resident_warps(name, si, order):
+    """A V1Merge batch with more queries than resident warps: by default the lean kernel runs every
+    query's upper-level descent first, orders the queries by their level-0 entry distance and then
+    searches level 0 from the stored entries (query_order -1: one pass in batch order). Either way
+    ids, distances and per-query counts (the descent's included) are the oracle's."""
+    k, ef, algo = golden_manifest()[name]["settings"][si]
+    q = load_golden(name)["queries"]
+    reps = -(-12000 // len(q))
+    big = np.ascontiguousarray(np.tile(q, (reps, 1)))
+    idx = _gpu_index(name)
+    idx.setLaunchConfig(query_order=order)
+    try:
+        idx.setQueryTimeParams({"efSearch": ef, "algoType": algo})
+        ids, d, cnt, st = idx.knnQueryBatchArrays(big, k, stats=True)
+    finally:
+        idx.setLaunchConfig()
+    oi, od, oc, ost = _oracle(name).search(q, k=k, ef=ef, algo=ALGO_CODES[algo])
+    np.testing.assert_array_equal(cnt, np.tile(oc, reps))
+    np.testing.assert_array_equal(ids, np.tile(oi, (reps, 1)))
+    np.testing.assert_array_equal(d.view(np.int32), np.tile(od, (reps, 1)).view(np.int32))
+    np.testing.assert_array_equal(st, np.tile(ost, (reps, 1)))
+
+
+def test_cuda_graph_replays_the_split_search():
+    """NMSG_CUDA_GRAPH with a batch larger than the resident warps: the captured sequence (descent,
+    order, level 0) replays with the results of the uncaptured search."""
+    import torch
+
+    from nmslib_b200 import _capi
+    idx = _gpu_index("c1_l2_d128")
+    lib = _capi.load()
+    q = np.ascontiguousarray(np.tile(load_golden("c1_l2_d128")["queries"], (12, 1)))
+    nq, dim = q.shape
+    dq = torch.from_numpy(q).cuda()
+    idx.setQueryTimeParams({"efSearch": 64})
+    want = idx.knnQueryBatchArrays(q, 10)
+    for _ in range(3):
+        ids = torch.full((nq, 10), -7, dtype=torch.int32, device="cuda")
+        d = torch.zeros((nq, 10), dtype=torch.float32, device="cuda")
+        c = torch.zeros((nq,), dtype=torch.int32, device="cuda")
+        rc = lib.nmsg_knn_batch(idx._h, dq.data_ptr(), nq, dim, 10, None, None, 10, ids.data_ptr(),
+                                d.data_ptr(), c.data_ptr(), None,
+                                _capi.FLAG_DEVICE_PTRS | _capi.FLAG_CUDA_GRAPH, None)
+        assert rc == 0, _capi.last_error()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(ids.cpu().numpy(), want[0])
+        np.testing.assert_array_equal(d.cpu().numpy().view(np.int32), want[1].view(np.int32))
+        np.testing.assert_array_equal(c.cpu().numpy(), want[2])
