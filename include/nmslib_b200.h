@@ -190,6 +190,10 @@ typedef struct nmsg_launch_config {
                                 of up to 64 ids; other batches run one query per warp */
   int32_t row_copy;          /* that kernel's row staging: 0 = automatic, 1 = 16-byte asynchronous
                                 copies spread over the lanes, 2 = one bulk copy (TMA unit) per row */
+  int32_t query_order;       /* V1Merge batches of one efSearch on the lean kernel with more queries
+                                than resident warps: 0 = automatic (every query's upper-level descent
+                                first, then level 0 with the queries that enter it farthest from
+                                their query first), -1 = one pass in batch order */
 } nmsg_launch_config;
 
 /* Set (cfg != NULL) or reset to automatic (cfg == NULL) the launch shape used by later

@@ -33,7 +33,7 @@ class LaunchConfig(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int32), ("rows_per_group", ctypes.c_int32),
                 ("stage_rows", ctypes.c_int32), ("visited_hash_log2", ctypes.c_int32),
                 ("plain_slots", ctypes.c_int32), ("queries_per_warp", ctypes.c_int32),
-                ("row_copy", ctypes.c_int32)]
+                ("row_copy", ctypes.c_int32), ("query_order", ctypes.c_int32)]
 
 
 _lib = None

@@ -130,6 +130,15 @@ struct SearchArgs {
   uint8_t* visited = nullptr;       // [num_slots][visited_pitch] epoch bytes
   int64_t visited_pitch = 0;
   uint8_t* epochs = nullptr;        // [num_slots]
+  // Split lean search (split 1: upper-level descent only; 2: level 0 from the stored entries):
+  // where each query enters level 0, its distance there (the work order key), the descent's
+  // counts (distances, upper-level list scans, list ints) and the range of the keys.
+  int split = 0;
+  int32_t* entry_node = nullptr;    // [nq]
+  float* entry_dist = nullptr;      // [nq]
+  int32_t* entry_stats = nullptr;   // [nq][3]
+  uint32_t* entry_range = nullptr;  // [2]: smallest and largest ordered key
+  int32_t* entry_order = nullptr;   // [nq]: the level-0 pass's work order (largest entry distance first)
   int32_t* slot_locks = nullptr;    // [num_slots] (one-query-per-block kernel only)
   int num_slots = 0;
   uint2* old_heap = nullptr;        // [num_slots][old_heap_cap] SearchOld candidate heaps

@@ -100,12 +100,13 @@ struct nmsg_index {
   nmsg::DevBuf vecs, norms, l0, up_off, up_links, ext_id;
   // search scratch (grown on demand)
   nmsg::DevBuf visited, epochs, locks, old_heap, counter, status, order, kq, efq;
+  nmsg::DevBuf entry;       // split lean search: entry nodes, distances, counts, key range, order
   nmsg::DevBuf q_stage, ids_stage, dists_stage, counts_stage, stats_stage;
   int slots = 0;            // slots covered by visited/epochs/locks
   int64_t old_cap = 0;      // entries per slot in old_heap
   int64_t resident_bytes = 0;
   int last_status = NMSG_OK;
-  nmsg_launch_config cfg{0, 0, 0, 0, 0, 0, 0};
+  nmsg_launch_config cfg{0, 0, 0, 0, 0, 0, 0, 0};
   nmsg::BruteForceState* bf = nullptr;  // brute-force data, built on first use
   cudaGraphExec_t graph_exec = nullptr;  // last captured device-pointer search (NMSG_CUDA_GRAPH)
   cudaStream_t capture_stream = nullptr;

@@ -277,8 +277,18 @@ __device__ bool lean_query(const SearchArgs& a, LeanWarp& w, int64_t qi, uint8_t
   int pos[NCH], id[NCH];
   // ---- the entry point, then the greedy descent (hnsw_distfunc_opt.cc:168-198): at each level
   // move to the earliest list entry whose distance is strictly below every earlier one, while
-  // one is below the current distance
+  // one is below the current distance. In the level-0 pass of a split search the descent's end
+  // (and its counts) come from the descent pass instead.
   int cur = ix.enterpoint;
+  float curdist = 0.0f;
+  if (a.split == 2) {
+    cur = __ldg(a.entry_node + qi);
+    curdist = __ldg(a.entry_dist + qi);
+    w.st_dist = __ldg(a.entry_stats + 3 * qi + 0);
+    w.st_greedy = __ldg(a.entry_stats + 3 * qi + 1);
+    w.st_list_ints = __ldg(a.entry_stats + 3 * qi + 2);
+    if (cur < 0 || cur >= ix.n) return false;  // the descent pass gave up on this query
+  } else {
 #pragma unroll
   for (int h = 0; h < NCH; ++h) {
     has[h] = h == 0 && lane == 0;
@@ -286,7 +296,7 @@ __device__ bool lean_query(const SearchArgs& a, LeanWarp& w, int64_t qi, uint8_t
     id[h] = cur;
   }
   if (!lean_rows<NF, HALF, SP, NCH>(ix, w, q, has, pos, id, 1)) return false;
-  float curdist = w.nb_d[0];
+  curdist = w.nb_d[0];
   w.st_dist += 1;
   for (int lev = ix.maxlevel; lev > 0; --lev) {
     while (true) {
@@ -332,6 +342,21 @@ __device__ bool lean_query(const SearchArgs& a, LeanWarp& w, int64_t qi, uint8_t
       cur = bid;
       curdist = best;
     }
+  }
+  if (a.split == 1) {  // the descent pass: record where level 0 starts, and the key it is ordered by
+    if (lane == 0) {
+      a.entry_node[qi] = cur;
+      a.entry_dist[qi] = curdist;
+      a.entry_stats[3 * qi + 0] = w.st_dist;
+      a.entry_stats[3 * qi + 1] = w.st_greedy;
+      a.entry_stats[3 * qi + 2] = w.st_list_ints;
+      const uint32_t key = ordered_key(curdist);
+      atomicMin(a.entry_range + 0, key);
+      atomicMax(a.entry_range + 1, key);
+    }
+    __syncwarp();
+    return true;
+  }
   }
   // ---- level 0 (hnsw_distfunc_opt.cc:200-283)
   const int cap = max(ef, k);
@@ -488,18 +513,21 @@ __global__ void __launch_bounds__(128, 8) search_lean_kernel(SearchArgs a) {
     item = __shfl_sync(kFull, item, 0);
     if (item >= a.nq) break;
     const int64_t qi = a.order ? a.order[item] : item;
-    // next epoch of this slot's visited bytes; cleared when the byte wraps (hnsw.h:582-589)
+    // next epoch of this slot's visited bytes; cleared when the byte wraps (hnsw.h:582-589). The
+    // descent pass of a split search touches no visited set.
     int ep = 0;
-    if (lane == 0) ep = a.epochs[slot] + 1;
-    ep = __shfl_sync(kFull, ep, 0);
-    if (ep == 256) {
-      uint4* p = reinterpret_cast<uint4*>(w.vis);
-      const int64_t n16 = a.visited_pitch / 16;
-      for (int64_t t = lane; t < n16; t += 32) p[t] = make_uint4(0, 0, 0, 0);
-      ep = 1;
-      __syncwarp();
+    if (a.split != 1) {
+      if (lane == 0) ep = a.epochs[slot] + 1;
+      ep = __shfl_sync(kFull, ep, 0);
+      if (ep == 256) {
+        uint4* p = reinterpret_cast<uint4*>(w.vis);
+        const int64_t n16 = a.visited_pitch / 16;
+        for (int64_t t = lane; t < n16; t += 32) p[t] = make_uint4(0, 0, 0, 0);
+        ep = 1;
+        __syncwarp();
+      }
+      if (lane == 0) a.epochs[slot] = (uint8_t)ep;
     }
-    if (lane == 0) a.epochs[slot] = (uint8_t)ep;
     if (!lean_query<NF, HALF, SP, NCH>(a, w, qi, (uint8_t)ep)) {
       if (lane == 0) set_status(a.status, NMSG_ERR_TIMEOUT);
       return;

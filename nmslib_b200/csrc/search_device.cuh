@@ -26,6 +26,13 @@ __device__ __forceinline__ uint2 make_item(float key, int id, bool used) {
 
 __device__ __forceinline__ void set_status(int32_t* status, int code) { atomicCAS(status, 0, code); }
 
+// A float as an unsigned key with the same order (negative values flipped entirely, positive ones
+// with the sign bit set), so that atomicMin / atomicMax and integer buckets order floats.
+__device__ __forceinline__ uint32_t ordered_key(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
 __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
