@@ -620,12 +620,13 @@ def aux_workload(which, device=0, serving_rates=(250e3, 500e3, 1e6)):
         k = rng.choice([1, 10, 100], nq).astype(np.int32)
         ef = rng.integers(64, 1025, nq).astype(np.int32)
         dt, (ids, d, cnt) = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
-        # the same launch with the 3840-byte rows staged in shared memory, 8 per round, by one bulk
-        # copy (TMA unit) per row or by 16-byte copies spread over the lanes, against the default
-        # (rows gathered into registers, one per 8-lane group)
-        row_copy = {"register_rows_ms": round(dt * 1e3, 2)}
+        # the same launch with each way of fetching the 3840-byte rows: staged in shared memory 8
+        # per round by one bulk copy (TMA unit) per row (the default) or by 16-byte copies spread
+        # over the lanes, or gathered into registers, one row per 8-lane group
+        row_copy = {"default_ms": round(dt * 1e3, 2)}
         for label, cfg in (("staged_bulk_ms", dict(stage_rows=8, row_copy=2)),
-                           ("staged_cp16_ms", dict(stage_rows=8, row_copy=1))):
+                           ("staged_cp16_ms", dict(stage_rows=8, row_copy=1)),
+                           ("register_rows_ms", dict(stage_rows=-1, rows_per_group=1))):
             index.setLaunchConfig(**cfg)
             dts, (ids_s, _, _) = timed(lambda: index.knnQueryBatchArrays(queries, k, ef=ef))
             index.setLaunchConfig()
