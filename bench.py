@@ -293,8 +293,9 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ ncu traffic record
 def recorded_traffic():
-    """DRAM bytes per launch of the search kernel from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "hnsw_search_batched_c2.md")
+    """DRAM bytes of one 10K-query search step (the lean kernel's descent and level-0 launches)
+    from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "search_lean_kernel_c2.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
