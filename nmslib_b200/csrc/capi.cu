@@ -624,9 +624,10 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
     }
   }
   a.nbpad = plan.nbpad;
-  // Split lean search: worth it once the batch outnumbers the resident warps (some warps then run
-  // several queries, and which queries start last decides when the batch ends).
-  if (plan.lean && !plain && !a.order && nq > slots && h->cfg.query_order != -1) {
+  // Split search: worth it once the batch outnumbers the resident warps (some warps then run
+  // several queries, and which queries start last decides when the batch ends). V1Merge batches of
+  // one efSearch on the one-query-per-warp kernels.
+  if ((plan.lean || (plan.ctx == 1 && !any_old)) && !plain && !a.order && nq > slots && h->cfg.query_order != -1) {
     const size_t words = (size_t)nq * 6 + 4;  // node, distance, 3 counts, order; range
     NMSG_CUDA(h->entry.ensure(words * 4, false), "cudaMalloc(level-0 entries)");
     int32_t* e = h->entry.as<int32_t>();

@@ -834,18 +834,21 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
     w.phase = bar_phase;
   }
 
-  // next epoch of this slot's visited array; clear it when the byte wraps (hnsw.h:582-589)
+  // next epoch of this slot's visited array; clear it when the byte wraps (hnsw.h:582-589). The
+  // descent pass of a split search touches no visited set.
   int ep = 0;
-  if (lane == 0) ep = a.epochs[slot] + 1;
-  ep = __shfl_sync(kFull, ep, 0);
-  if (ep == 256) {
-    uint4* p = reinterpret_cast<uint4*>(w.vis);
-    const int64_t n16 = a.visited_pitch / 16;
-    for (int64_t t = lane; t < n16; t += 32) p[t] = make_uint4(0, 0, 0, 0);
-    ep = 1;
-    __syncwarp();
+  if (a.split != 1) {
+    if (lane == 0) ep = a.epochs[slot] + 1;
+    ep = __shfl_sync(kFull, ep, 0);
+    if (ep == 256) {
+      uint4* p = reinterpret_cast<uint4*>(w.vis);
+      const int64_t n16 = a.visited_pitch / 16;
+      for (int64_t t = lane; t < n16; t += 32) p[t] = make_uint4(0, 0, 0, 0);
+      ep = 1;
+      __syncwarp();
+    }
+    if (lane == 0) a.epochs[slot] = (uint8_t)ep;
   }
-  if (lane == 0) a.epochs[slot] = (uint8_t)ep;
   w.epoch = (uint8_t)ep;
 
   const int k = a.k_per_q ? a.k_per_q[qi] : a.k_default;
@@ -853,19 +856,47 @@ __device__ void run_query(const SearchArgs& a, char* wsmem, int slot, int64_t qi
   load_query(a, w.q, qi);
   int cur;
   float curdist;
-  greedy_descent<R>(a, w, cur, curdist);
-  const bool use_old = a.algo == NMSG_ALGO_OLD || (a.algo == NMSG_ALGO_HYBRID && ef >= 1000);
-  if (OLD && use_old) {
-    search_old<R>(a, w, qi, k, ef, cur, curdist, a.old_heap + (int64_t)slot * a.old_heap_cap);
+  bool search = true;
+  if (a.split == 2) {  // level 0 from where the descent pass ended, with its counts
+    cur = __ldg(a.entry_node + qi);
+    curdist = __ldg(a.entry_dist + qi);
+    w.st_dist = __ldg(a.entry_stats + 3 * qi + 0);
+    w.st_greedy = __ldg(a.entry_stats + 3 * qi + 1);
+    w.st_bytes = __ldg(a.entry_stats + 3 * qi + 2);
+    if (cur < 0 || cur >= ix.n) {  // the descent pass gave up on this query
+      search = false;
+      w.failed = true;
+    }
   } else {
-    search_v1merge<R>(a, w, qi, k, ef, cur, curdist);
+    greedy_descent<R>(a, w, cur, curdist);
+    if (a.split == 1) {  // the descent pass: where level 0 starts and the key it is ordered by
+      if (lane == 0 && !w.failed) {
+        a.entry_node[qi] = cur;
+        a.entry_dist[qi] = curdist;
+        a.entry_stats[3 * qi + 0] = w.st_dist;
+        a.entry_stats[3 * qi + 1] = w.st_greedy;
+        a.entry_stats[3 * qi + 2] = (int32_t)w.st_bytes;
+        const uint32_t key = ordered_key(curdist);
+        atomicMin(a.entry_range + 0, key);
+        atomicMax(a.entry_range + 1, key);
+      }
+      search = false;
+    }
+  }
+  if (search) {
+    const bool use_old = a.algo == NMSG_ALGO_OLD || (a.algo == NMSG_ALGO_HYBRID && ef >= 1000);
+    if (OLD && use_old) {
+      search_old<R>(a, w, qi, k, ef, cur, curdist, a.old_heap + (int64_t)slot * a.old_heap_cap);
+    } else {
+      search_v1merge<R>(a, w, qi, k, ef, cur, curdist);
+    }
   }
   bar_phase = w.phase;
   if (w.failed && lane == 0) {  // a row copy gave up: the query's results are not trusted
     set_status(a.status, NMSG_ERR_TIMEOUT);
     a.counts[qi] = 0;
   }
-  if (a.stats && lane == 0) {
+  if (a.stats && lane == 0 && a.split != 1) {
     a.stats[qi * 4 + 0] = w.st_dist;
     a.stats[qi * 4 + 1] = w.st_expand;
     a.stats[qi * 4 + 2] = w.st_greedy;
@@ -2052,7 +2083,7 @@ int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, in
   const int smem = a.warp_smem * (plain ? 1 : warps_per_block);
   const int rc = allow_max_smem((const void*)kern);
   if (rc != 0) return rc;
-  if (a.lean && !plain && a.entry_node) {
+  if (!plain && a.entry_node) {
     // split: the upper-level descent of every query, the order, then level 0 in that order
     cudaStream_t st = (cudaStream_t)stream;
     SearchArgs d = a;

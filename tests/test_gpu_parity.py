@@ -383,12 +383,14 @@ def test_staged_wide_rows_many_queries_per_warp(row_copy):
 
 @pytest.mark.parametrize("order", [0, -1], ids=["split", "one-pass"])
 @pytest.mark.parametrize("name,si", [("c1_l2_d128", 0), ("c1_l2_d128", 3), ("c1_l2_d128", 6), ("sift_l2_ties", 0),
-                                     ("dup_l2_d16", 2), ("tiny_cos_d48", 0)])
+                                     ("dup_l2_d16", 2), ("tiny_cos_d48", 0), ("cos_d100", 0), ("negdot_d960", 0),
+                                     ("l1_d22", 0), ("linf_d128", 0), ("tiny_l2_d20_sqids", 0)])
 def test_batches_larger_than_the_resident_warps(name, si, order):
-    """A V1Merge batch with more queries than resident warps: by default the lean kernel runs every
-    query's upper-level descent first, orders the queries by their level-0 entry distance and then
-    searches level 0 from the stored entries (query_order -1: one pass in batch order). Either way
-    ids, distances and per-query counts (the descent's included) are the oracle's."""
+    """A V1Merge batch with more queries than resident warps: by default the lean kernel (and the
+    general kernel for the other row shapes and distances) runs every query's upper-level descent
+    first, orders the queries by their level-0 entry distance and then searches level 0 from the
+    stored entries (query_order -1: one pass in batch order). Either way ids, distances and
+    per-query counts (the descent's included) are the oracle's."""
     k, ef, algo = golden_manifest()[name]["settings"][si]
     q = load_golden(name)["queries"]
     reps = -(-12000 // len(q))
