@@ -365,6 +365,10 @@ __global__ void __launch_bounds__(Roles<MODE>::kThreads, 1)
         const int buf = tcount & 1;
         __syncwarp();  // every lane is done with the previous tile's norms
         if (lane < CW / 4) reinterpret_cast<float4*>(snw)[lane] = nrm_next;
+        // the smallest |x|^2 of each 16-column group: lane 4g holds group g's
+        float gmin = fminf(fminf(nrm_next.x, nrm_next.y), fminf(nrm_next.z, nrm_next.w));
+        gmin = fminf(gmin, __shfl_xor_sync(0xffffffffu, gmin, 1));
+        gmin = fminf(gmin, __shfl_xor_sync(0xffffffffu, gmin, 2));
         if (vt + 1 < t1) nrm_next = __ldg(xn4 + (size_t)(t + a.tile_step) * (BN / 4));
         __syncwarp();
         ok = mbar_wait(&acc_full[buf], accphase[buf]);
@@ -388,26 +392,31 @@ __global__ void __launch_bounds__(Roles<MODE>::kThreads, 1)
             if (lane == 0) mbar_arrive(&acc_empty[buf]);  // this warp's part of the accumulator is read
           }
           const int col0 = t * BN + part * CW + c * 16;
-          // keys: ks * acc - xnorm2, as in the sample pass; rows past the base have key -inf
-          float v[16];
-          const float4* nv = reinterpret_cast<const float4*>(snw + c * 16);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const float4 x4 = nv[j];  // same address in every lane: a broadcast
-            v[4 * j + 0] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 0]), -x4.x);
-            v[4 * j + 1] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 1]), -x4.y);
-            v[4 * j + 2] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 2]), -x4.z);
-            v[4 * j + 3] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 3]), -x4.w);
-          }
+          // An upper bound of the group's keys (ks * acc - xnorm2): ks * (largest acc) - (smallest
+          // xnorm2), rounded as one FMA. The exact sum is at least every column's, and rounding to
+          // nearest is monotone, so no key of the group exceeds the bound: below tau, the group
+          // has no hit and its keys are never formed.
           float m[8];
 #pragma unroll
-          for (int i = 0; i < 8; ++i) m[i] = fmaxf(v[i], v[i + 8]);
+          for (int i = 0; i < 8; ++i) m[i] = fmaxf(__uint_as_float(cur[i]), __uint_as_float(cur[i + 8]));
 #pragma unroll
           for (int w = 4; w > 0; w >>= 1)
 #pragma unroll
             for (int i = 0; i < w; ++i) m[i] = fmaxf(m[i], m[i + w]);
+          const float bound = __fmaf_rn(ks, m[0], -__shfl_sync(0xffffffffu, gmin, 4 * c));
           // one warp vote first: the common case (no row of the warp passes) skips the rest
-          if (__any_sync(0xffffffffu, m[0] >= thr)) {
+          if (__any_sync(0xffffffffu, bound >= thr)) {
+            // the keys, as in the sample pass (rows past the base have key -inf)
+            float v[16];
+            const float4* nv = reinterpret_cast<const float4*>(snw + c * 16);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const float4 x4 = nv[j];  // same address in every lane: a broadcast
+              v[4 * j + 0] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 0]), -x4.x);
+              v[4 * j + 1] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 1]), -x4.y);
+              v[4 * j + 2] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 2]), -x4.z);
+              v[4 * j + 3] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 3]), -x4.w);
+            }
             // this row's hits as a bit mask built with selects, then one store pair per hit in a
             // loop whose trip count is the warp's largest hit count, plain stores into the row's list
             unsigned hm = 0;
