@@ -290,73 +290,73 @@ __device__ bool lean_query(const SearchArgs& a, LeanWarp& w, int64_t qi, uint8_t
     if (cur < 0 || cur >= ix.n) return false;  // the descent pass gave up on this query
   } else {
 #pragma unroll
-  for (int h = 0; h < NCH; ++h) {
-    has[h] = h == 0 && lane == 0;
-    pos[h] = 0;
-    id[h] = cur;
-  }
-  if (!lean_rows<NF, HALF, SP, NCH>(ix, w, q, has, pos, id, 1)) return false;
-  curdist = w.nb_d[0];
-  w.st_dist += 1;
-  for (int lev = ix.maxlevel; lev > 0; --lev) {
-    while (true) {
-      const int32_t* lst = ix.up_links + __ldg(ix.up_off + cur) + (int64_t)(ix.maxM + 1) * (lev - 1);
-      const int cnt = __ldg(lst);
+    for (int h = 0; h < NCH; ++h) {
+      has[h] = h == 0 && lane == 0;
+      pos[h] = 0;
+      id[h] = cur;
+    }
+    if (!lean_rows<NF, HALF, SP, NCH>(ix, w, q, has, pos, id, 1)) return false;
+    curdist = w.nb_d[0];
+    w.st_dist += 1;
+    for (int lev = ix.maxlevel; lev > 0; --lev) {
+      while (true) {
+        const int32_t* lst = ix.up_links + __ldg(ix.up_off + cur) + (int64_t)(ix.maxM + 1) * (lev - 1);
+        const int cnt = __ldg(lst);
 #pragma unroll
-      for (int h = 0; h < NCH; ++h) {
-        const int t = 32 * h + lane;
-        has[h] = t < cnt;
-        pos[h] = t;
-        id[h] = has[h] ? __ldg(lst + 1 + t) : 0;
-      }
-      if (!lean_rows<NF, HALF, SP, NCH>(ix, w, q, has, pos, id, cnt)) return false;
-      w.st_greedy += 1;
-      w.st_dist += cnt;
-      w.st_list_ints += 1 + cnt;
-      float best = curdist;
-      int bpos = 0x7fffffff, bid = 0;
+        for (int h = 0; h < NCH; ++h) {
+          const int t = 32 * h + lane;
+          has[h] = t < cnt;
+          pos[h] = t;
+          id[h] = has[h] ? __ldg(lst + 1 + t) : 0;
+        }
+        if (!lean_rows<NF, HALF, SP, NCH>(ix, w, q, has, pos, id, cnt)) return false;
+        w.st_greedy += 1;
+        w.st_dist += cnt;
+        w.st_list_ints += 1 + cnt;
+        float best = curdist;
+        int bpos = 0x7fffffff, bid = 0;
 #pragma unroll
-      for (int h = 0; h < NCH; ++h) {
-        if (has[h]) {
-          const float d = w.nb_d[pos[h]];
-          if (d < best) {
-            best = d;
-            bpos = pos[h];
-            bid = id[h];
+        for (int h = 0; h < NCH; ++h) {
+          if (has[h]) {
+            const float d = w.nb_d[pos[h]];
+            if (d < best) {
+              best = d;
+              bpos = pos[h];
+              bid = id[h];
+            }
           }
         }
-      }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const float ob = __shfl_xor_sync(kFull, best, o);
-        const int op = __shfl_xor_sync(kFull, bpos, o);
-        const int oi = __shfl_xor_sync(kFull, bid, o);
-        if (ob < best || (ob == best && op < bpos)) {
-          best = ob;
-          bpos = op;
-          bid = oi;
+        for (int o = 16; o > 0; o >>= 1) {
+          const float ob = __shfl_xor_sync(kFull, best, o);
+          const int op = __shfl_xor_sync(kFull, bpos, o);
+          const int oi = __shfl_xor_sync(kFull, bid, o);
+          if (ob < best || (ob == best && op < bpos)) {
+            best = ob;
+            bpos = op;
+            bid = oi;
+          }
         }
+        __syncwarp();
+        if (!(bpos != 0x7fffffff && best < curdist)) break;
+        cur = bid;
+        curdist = best;
+      }
+    }
+    if (a.split == 1) {  // the descent pass: record where level 0 starts, and the key it is ordered by
+      if (lane == 0) {
+        a.entry_node[qi] = cur;
+        a.entry_dist[qi] = curdist;
+        a.entry_stats[3 * qi + 0] = w.st_dist;
+        a.entry_stats[3 * qi + 1] = w.st_greedy;
+        a.entry_stats[3 * qi + 2] = w.st_list_ints;
+        const uint32_t key = ordered_key(curdist);
+        atomicMin(a.entry_range + 0, key);
+        atomicMax(a.entry_range + 1, key);
       }
       __syncwarp();
-      if (!(bpos != 0x7fffffff && best < curdist)) break;
-      cur = bid;
-      curdist = best;
+      return true;
     }
-  }
-  if (a.split == 1) {  // the descent pass: record where level 0 starts, and the key it is ordered by
-    if (lane == 0) {
-      a.entry_node[qi] = cur;
-      a.entry_dist[qi] = curdist;
-      a.entry_stats[3 * qi + 0] = w.st_dist;
-      a.entry_stats[3 * qi + 1] = w.st_greedy;
-      a.entry_stats[3 * qi + 2] = w.st_list_ints;
-      const uint32_t key = ordered_key(curdist);
-      atomicMin(a.entry_range + 0, key);
-      atomicMax(a.entry_range + 1, key);
-    }
-    __syncwarp();
-    return true;
-  }
   }
   // ---- level 0 (hnsw_distfunc_opt.cc:200-283)
   const int cap = max(ef, k);
