@@ -602,12 +602,29 @@ __device__ __forceinline__ bool better(DF ka, int ia, DF kb, int ib) {
   return df_greater(ka, kb) || (ka.hi == kb.hi && ka.lo == kb.lo && ia < ib);
 }
 
-// Exact key of one (query, row) pair computed by a single lane (sequential over the dimension).
+// Exact key of one (query, row) pair computed by a single lane (sequential over the dimension), in
+// FP64: a product of two floats is exact in a double and each FMA rounds the running sum once (a
+// relative error of about dim * 2^-53, far below the BF16 bound eps), returned as a double-float
+// pair (hi = the double rounded to float, lo = the rest rounded to float) like the other keys.
 __device__ DF exact_key_lane(const float* __restrict__ q, const float* __restrict__ x, int dim, bool l2, DF xnorm) {
-  DF acc{0.0f, 0.0f};
-  for (int e = 0; e < dim; ++e) acc = df_add_df(acc, df_mul_ff(q[e], __ldg(x + e)));
-  if (l2) return df_add_df(DF{__fmul_rn(2.0f, acc.hi), __fmul_rn(2.0f, acc.lo)}, DF{-xnorm.hi, -xnorm.lo});
-  return acc;
+  double acc = 0.0;
+  if ((dim & 3) == 0) {  // rows and queries start on 16-byte boundaries
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+    for (int e = 0; e < dim / 4; ++e) {
+      const float4 a = q4[e];
+      const float4 b = __ldg(x4 + e);
+      acc = fma((double)a.x, (double)b.x, acc);
+      acc = fma((double)a.y, (double)b.y, acc);
+      acc = fma((double)a.z, (double)b.z, acc);
+      acc = fma((double)a.w, (double)b.w, acc);
+    }
+  } else {
+    for (int e = 0; e < dim; ++e) acc = fma((double)q[e], (double)__ldg(x + e), acc);
+  }
+  if (l2) acc = fma(2.0, acc, -((double)xnorm.hi + (double)xnorm.lo));
+  const float hi = __double2float_rn(acc);
+  return DF{hi, __double2float_rn(acc - (double)hi)};
 }
 
 // One warp per query:
