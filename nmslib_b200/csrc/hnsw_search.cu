@@ -2036,10 +2036,12 @@ namespace {
 // filled (the order inside a bucket is arbitrary; results do not depend on the order).
 constexpr int kOrderBuckets = 2048;
 
-__device__ __forceinline__ int order_bucket(float v, uint32_t lo, uint32_t hi) {
+// Bucket of a key, largest keys in bucket 0; scale = (kOrderBuckets - 1) / (hi - lo). The same
+// float arithmetic in both passes over the keys, so a key lands in the same bucket each time.
+__device__ __forceinline__ int order_bucket(float v, uint32_t lo, uint32_t hi, float scale) {
   const uint32_t k = min(max(ordered_key(v), lo), hi);
-  const uint64_t span = hi > lo ? (uint64_t)(hi - lo) : 1;
-  return kOrderBuckets - 1 - (int)(((uint64_t)(k - lo) * (kOrderBuckets - 1)) / span);
+  const int b = min((int)(__uint2float_rz(k - lo) * scale), kOrderBuckets - 1);
+  return kOrderBuckets - 1 - b;
 }
 
 __global__ void __launch_bounds__(1024) order_by_entry_kernel(const float* __restrict__ key, int64_t nq,
@@ -2049,7 +2051,8 @@ __global__ void __launch_bounds__(1024) order_by_entry_kernel(const float* __res
   for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) cnt[b] = 0;
   __syncthreads();
   const uint32_t lo = range[0], hi = range[1];
-  for (int64_t i = threadIdx.x; i < nq; i += blockDim.x) atomicAdd(&cnt[order_bucket(key[i], lo, hi)], 1);
+  const float scale = (float)(kOrderBuckets - 1) / __uint2float_ru(hi > lo ? hi - lo : 1u);
+  for (int64_t i = threadIdx.x; i < nq; i += blockDim.x) atomicAdd(&cnt[order_bucket(key[i], lo, hi, scale)], 1);
   __syncthreads();
   if (threadIdx.x < 32) {  // exclusive scan: each lane a run of 64 buckets, then across the lanes
     constexpr int kRun = kOrderBuckets / 32;
@@ -2071,7 +2074,7 @@ __global__ void __launch_bounds__(1024) order_by_entry_kernel(const float* __res
   }
   __syncthreads();
   for (int64_t i = threadIdx.x; i < nq; i += blockDim.x)
-    order[atomicAdd(&cnt[order_bucket(key[i], lo, hi)], 1)] = (int32_t)i;
+    order[atomicAdd(&cnt[order_bucket(key[i], lo, hi, scale)], 1)] = (int32_t)i;
 }
 
 }  // namespace
