@@ -163,3 +163,22 @@ def test_sift_rejects_float_paths():
     assert rc == _capi.ERR_UNSUPPORTED
     with pytest.raises(ValueError):
         idx.knnQueryBatchArrays(np.zeros((2, 64), np.uint8), 5)
+
+
+@pytest.mark.parametrize("name,si", [c for c in _cases() if _manifest()[c[0]]["settings"][c[1]][2] != "old"
+                                     and _manifest()[c[0]]["settings"][c[1]][1] < 1000])
+def test_sift_batch_larger_than_the_resident_warps(name, si):
+    """A V1Merge batch of uint8 queries with more queries than resident warps (descent pass, order by
+    entry distance, level-0 pass): ids, int distances and per-query counts are the oracle's."""
+    k, ef, algo = _manifest()[name]["settings"][si]
+    q = np.load(os.path.join(HERE, name + ".npz"))["queries"]
+    reps = -(-12000 // len(q))
+    big = np.ascontiguousarray(np.tile(q, (reps, 1)))
+    idx = _index(name)
+    idx.setQueryTimeParams({"efSearch": ef, "algoType": algo})
+    ids, d, cnt, st = idx.knnQueryBatchArrays(big, k, stats=True)
+    oi, od, oc, ost = _oracle(name).search(q, k, ef, ALGO[algo], stats=True)
+    np.testing.assert_array_equal(cnt, np.tile(oc, reps))
+    np.testing.assert_array_equal(ids, np.tile(oi, (reps, 1)))
+    np.testing.assert_array_equal(d, np.tile(od, (reps, 1)))
+    np.testing.assert_array_equal(st, np.tile(ost, (reps, 1)))
