@@ -107,7 +107,7 @@ struct nmsg_server {
     epochs.release();
   }
 
-  // Launch request r on lane li (worker thread, mu not held for the CUDA calls).
+  // Launch request r on lane li (worker thread, mu held).
   int launch(int li, Request& r) {
     Lane& l = lanes[li];
     const DevIndex& d = h->dev;
@@ -240,7 +240,9 @@ struct nmsg_server {
         if (in_flight == 0 && queue.empty()) {
           cv_work.wait_for(lk, std::chrono::milliseconds(50));
         } else {
-          // work on the device: poll again shortly without holding the lock
+          // work on the device: poll again shortly without holding the lock (polling at once,
+          // with a yield only, measured far worse: the worker took the lock back before the
+          // threads submitting requests could, p50 1.74 -> 5.1 ms at 500K q/s offered)
           lk.unlock();
           std::this_thread::sleep_for(std::chrono::microseconds(5));
           lk.lock();
