@@ -123,6 +123,13 @@ __device__ __forceinline__ int next_active_item(const GemmArgs& a, int item, int
   return item;
 }
 
+// The largest of three floats in one instruction (max.f32 with three sources).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
 // v[i] of 16 values for a lane-dependent i, by four levels of selects.
 __device__ __forceinline__ float pick16(const float (&v)[16], int i) {
   float a[8];
@@ -374,36 +381,20 @@ __global__ void __launch_bounds__(Roles<MODE>::kThreads, 1)
         ok = mbar_wait(&acc_full[buf], accphase[buf]);
         accphase[buf] ^= 1;
         tc_fence_after();
-        // TMEM loads of the next 16 columns overlap the work on the current ones
-        const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + buf * BN + part * CW;
-        uint32_t ra[16];
-        tmem_ld16_issue(tb, ra);
-        tmem_ld_wait16(ra);
-#pragma unroll 1
-        for (int c = 0; c < CW / 16; ++c) {
-          uint32_t cur[16];
-#pragma unroll
-          for (int i = 0; i < 16; ++i) cur[i] = ra[i];
-          if (c + 1 < CW / 16) {
-            tmem_ld16_issue(tb + 16 * (c + 1), ra);
-          } else {
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[buf]);  // this warp's part of the accumulator is read
-          }
+        // the work on one 16-column group (cur: its accumulators)
+        auto group = [&](const uint32_t (&cur)[16], int c) {
           const int col0 = t * BN + part * CW + c * 16;
           // An upper bound of the group's keys (ks * acc - xnorm2): ks * (largest acc) - (smallest
           // xnorm2), rounded as one FMA. The exact sum is at least every column's, and rounding to
           // nearest is monotone, so no key of the group exceeds the bound: below tau, the group
-          // has no hit and its keys are never formed.
-          float m[8];
-#pragma unroll
-          for (int i = 0; i < 8; ++i) m[i] = fmaxf(__uint_as_float(cur[i]), __uint_as_float(cur[i + 8]));
-#pragma unroll
-          for (int w = 4; w > 0; w >>= 1)
-#pragma unroll
-            for (int i = 0; i < w; ++i) m[i] = fmaxf(m[i], m[i + w]);
-          const float bound = __fmaf_rn(ks, m[0], -__shfl_sync(0xffffffffu, gmin, 4 * c));
+          // has no hit and its keys are never formed. The maximum: three-input max instructions.
+          const float m0 = max3f(__uint_as_float(cur[0]), __uint_as_float(cur[1]), __uint_as_float(cur[2]));
+          const float m1 = max3f(__uint_as_float(cur[3]), __uint_as_float(cur[4]), __uint_as_float(cur[5]));
+          const float m2 = max3f(__uint_as_float(cur[6]), __uint_as_float(cur[7]), __uint_as_float(cur[8]));
+          const float m3 = max3f(__uint_as_float(cur[9]), __uint_as_float(cur[10]), __uint_as_float(cur[11]));
+          const float m4 = max3f(__uint_as_float(cur[12]), __uint_as_float(cur[13]), __uint_as_float(cur[14]));
+          const float mx = fmaxf(max3f(m0, m1, m2), max3f(m3, m4, __uint_as_float(cur[15])));
+          const float bound = __fmaf_rn(ks, mx, -__shfl_sync(0xffffffffu, gmin, 4 * c));
           // one warp vote first: the common case (no row of the warp passes) skips the rest
           if (__any_sync(0xffffffffu, bound >= thr)) {
             // the keys, as in the sample pass (rows past the base have key -inf)
@@ -435,7 +426,27 @@ __global__ void __launch_bounds__(Roles<MODE>::kThreads, 1)
             }
           }
           __syncwarp();
-          if (c + 1 < CW / 16) tmem_ld_wait16(ra);
+        };
+        // TMEM loads of the next 16 columns overlap the work on the current ones, the groups
+        // alternating between two register buffers (no copies between them)
+        const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + buf * BN + part * CW;
+        uint32_t ra[16], rb[16];
+        tmem_ld16_issue(tb, ra);
+        tmem_ld_wait16(ra);
+#pragma unroll 1
+        for (int c = 0; c < CW / 16; c += 2) {
+          tmem_ld16_issue(tb + 16 * (c + 1), rb);
+          group(ra, c);
+          tmem_ld_wait16(rb);
+          if (c + 2 < CW / 16) {
+            tmem_ld16_issue(tb + 16 * (c + 2), ra);
+          } else {  // every load of this tile has completed
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[buf]);  // this warp's part of the accumulator is read
+          }
+          group(rb, c + 1);
+          if (c + 2 < CW / 16) tmem_ld_wait16(ra);
         }
       }
       if (qvalid) a.list_cnt[list] = ncoll;
