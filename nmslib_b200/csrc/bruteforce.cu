@@ -487,23 +487,8 @@ __global__ void __launch_bounds__(Roles<MODE>::kThreads, 1)
         ok = mbar_wait(&acc_full[buf], accphase[buf]);
         accphase[buf] ^= 1;
         tc_fence_after();
-        // TMEM loads of the next group of 32 columns overlap the work on the current one
-        const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + buf * BN + half * (BN / HALVES);
-        uint32_t ra[32];
-        tmem_ld32_issue(tb, ra);
-        tmem_ld_wait(ra);
-#pragma unroll 1
-        for (int c = 0; c < BN / HALVES / 32; ++c) {
-          uint32_t cur[32];
-#pragma unroll
-          for (int i = 0; i < 32; ++i) cur[i] = ra[i];
-          if (c + 1 < BN / HALVES / 32) {
-            tmem_ld32_issue(tb + 32 * (c + 1), ra);
-          } else {
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[buf]);  // the accumulator is read out
-          }
+        // the work on one 32-column group (cur: its accumulators)
+        auto group = [&](const uint32_t (&cur)[32], int c) {
           const int col0 = t * BN + half * (BN / HALVES) + c * 32;
           // keys: ks * acc - xnorm2 (l2: 2 q.x - |x|^2, where 2 acc is exact so one FMA rounds
           // as the two-step form would; dot spaces: acc - 0). Rows past the base have
@@ -518,14 +503,12 @@ __global__ void __launch_bounds__(Roles<MODE>::kThreads, 1)
             v[4 * j + 2] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 2]), -x4.z);
             v[4 * j + 3] = __fmaf_rn(ks, __uint_as_float(cur[4 * j + 3]), -x4.w);
           }
-          float m[16];
+          // the group's largest key, with three-input max instructions
+          float m[10];
 #pragma unroll
-          for (int i = 0; i < 16; ++i) m[i] = fmaxf(v[i], v[i + 16]);
-#pragma unroll
-          for (int w = 8; w > 0; w >>= 1)
-#pragma unroll
-            for (int i = 0; i < w; ++i) m[i] = fmaxf(m[i], m[i + w]);
-          const float mx = m[0];
+          for (int i = 0; i < 10; ++i) m[i] = max3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+          const float mx = fmaxf(max3f(max3f(m[0], m[1], m[2]), max3f(m[3], m[4], m[5]), max3f(m[6], m[7], m[8])),
+                                 max3f(m[9], v[30], v[31]));
           if (a.per_column) {
             // small bases (the sample is all of it): every column is offered
             if ((mx > thr || nfill < CAND) && mx > -INFINITY) {
@@ -546,7 +529,27 @@ __global__ void __launch_bounds__(Roles<MODE>::kThreads, 1)
             list_offer(lk, li, nfill, thr, mx, col0 + arg);
           }
           __syncwarp();
-          if (c + 1 < BN / HALVES / 32) tmem_ld_wait(ra);
+        };
+        // TMEM loads of the next group of 32 columns overlap the work on the current one, the
+        // groups alternating between two register buffers (no copies between them)
+        const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + buf * BN + half * (BN / HALVES);
+        uint32_t ra[32], rb[32];
+        tmem_ld32_issue(tb, ra);
+        tmem_ld_wait(ra);
+#pragma unroll 1
+        for (int c = 0; c < BN / HALVES / 32; c += 2) {
+          tmem_ld32_issue(tb + 32 * (c + 1), rb);
+          group(ra, c);
+          tmem_ld_wait(rb);
+          if (c + 2 < BN / HALVES / 32) {
+            tmem_ld32_issue(tb + 32 * (c + 2), ra);
+          } else {  // every load of this tile has completed
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[buf]);  // the accumulator is read out
+          }
+          group(rb, c + 1);
+          if (c + 2 < BN / HALVES / 32) tmem_ld_wait(ra);
         }
       }
       if (qvalid) {
