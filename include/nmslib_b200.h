@@ -194,6 +194,11 @@ typedef struct nmsg_launch_config {
                                 than resident warps: 0 = automatic (every query's upper-level descent
                                 first, then level 0 with the queries that enter it farthest from
                                 their query first), -1 = one pass in batch order */
+  int32_t host_copy;         /* calls on host buffers (no NMSG_DEVICE_PTRS): 0 = automatic (pageable
+                                buffers of 512 KB and more go through page-locked staging that
+                                several host threads fill and empty, with full-rate DMAs in between;
+                                page-locked buffers are copied directly), 1 = copy the caller's
+                                buffers directly */
 } nmsg_launch_config;
 
 /* Set (cfg != NULL) or reset to automatic (cfg == NULL) the launch shape used by later
@@ -284,6 +289,12 @@ NMSG_API void nmsg_query_server_stop(nmsg_query_server* server);
 
 /* Device status of the last batch on this handle (NMSG_OK or a device-side error code). */
 NMSG_API int nmsg_last_device_status(const nmsg_index* index);
+
+/* Search kernels the last nmsg_knn_batch / nmsg_knn_batch_u8 call on this handle launched (under
+ * NMSG_CUDA_GRAPH: launched by the graph it replayed): 1 for one pass, 3 for a batch that runs the
+ * upper-level descent, the entry ordering and level 0 as separate passes; 0 when it launched none
+ * (an empty batch or index, or a call that failed before launching). */
+NMSG_API int nmsg_last_kernel_launches(const nmsg_index* index);
 
 NMSG_API const char* nmsg_last_error(void);
 

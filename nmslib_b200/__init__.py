@@ -212,12 +212,13 @@ class FloatIndex:
         _capi.check(_capi.load().nmsg_set_query_params(h, ef, _ALGOS[algo]))
 
     def setLaunchConfig(self, warps_per_block=0, rows_per_group=0, visited_hash_log2=0, stage_rows=0,
-                        plain_slots=0, queries_per_warp=0, row_copy=0, query_order=0):
+                        plain_slots=0, queries_per_warp=0, row_copy=0, query_order=0, host_copy=0):
         """Launch shape of the search kernels (0 = automatic); results do not depend on it, except
         that plain_slots below the resident block count makes one-query-per-block launches give up
-        with a timeout error (the bounded slot wait)."""
+        with a timeout error (the bounded slot wait). host_copy=1 copies host arrays directly
+        instead of through page-locked staging."""
         cfg = _capi.LaunchConfig(warps_per_block, rows_per_group, stage_rows, visited_hash_log2, plain_slots,
-                                 queries_per_warp, row_copy, query_order)
+                                 queries_per_warp, row_copy, query_order, host_copy)
         _capi.check(_capi.load().nmsg_set_launch_config(self._require(), ctypes.byref(cfg)))
 
     # ------------------------------------------------------------------ search

@@ -33,7 +33,7 @@ class LaunchConfig(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int32), ("rows_per_group", ctypes.c_int32),
                 ("stage_rows", ctypes.c_int32), ("visited_hash_log2", ctypes.c_int32),
                 ("plain_slots", ctypes.c_int32), ("queries_per_warp", ctypes.c_int32),
-                ("row_copy", ctypes.c_int32), ("query_order", ctypes.c_int32)]
+                ("row_copy", ctypes.c_int32), ("query_order", ctypes.c_int32), ("host_copy", ctypes.c_int32)]
 
 
 _lib = None
@@ -94,6 +94,8 @@ def load(path: str = LIB_PATH):
     lib.nmsg_set_launch_config.restype = ctypes.c_int
     lib.nmsg_last_device_status.argtypes = [P]
     lib.nmsg_last_device_status.restype = ctypes.c_int
+    lib.nmsg_last_kernel_launches.argtypes = [P]
+    lib.nmsg_last_kernel_launches.restype = ctypes.c_int
     lib.nmsg_build_index.argtypes = [P, I64, I32, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_uint64, ctypes.c_char_p]
     lib.nmsg_build_index.restype = ctypes.c_int

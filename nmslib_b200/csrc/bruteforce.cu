@@ -1077,7 +1077,8 @@ int scan_fallback(nmsg_index* h, const float* queries, int64_t nq, int dim, int 
   const float* qin = queries;
   if (!dev_ptrs) {
     BF_CUDA(s->h_q.ensure((size_t)nq * dim * 4, false), "cudaMalloc(query staging)");
-    BF_CUDA(cudaMemcpyAsync(s->h_q.p, queries, (size_t)nq * dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
+    const HostPiece up{s->h_q.p, queries, (size_t)nq * dim * 4};
+    BF_CUDA(copy_to_device(h->pin_in, h->cfg.host_copy == 0, &up, 1, st), "copy queries");
     qin = s->h_q.as<float>();
   }
   BF_CUDA(s->scr_key.ensure(n_part * 4, false), "cudaMalloc(scan lists)");
@@ -1099,11 +1100,12 @@ int scan_fallback(nmsg_index* h, const float* queries, int64_t nq, int dim, int 
     return bf_fail(NMSG_ERR_DEVICE, std::string("exact scan: ") + cudaGetErrorString((cudaError_t)rc) +
                                         (rc == (int)cudaErrorInvalidValue ? " (rows too wide for the scan)" : ""));
   if (!dev_ptrs) {
-    BF_CUDA(cudaMemcpyAsync(ids, o_ids, (size_t)nq * kmax * 4, cudaMemcpyDeviceToHost, st), "copy ids");
-    BF_CUDA(cudaMemcpyAsync(dists, o_d, (size_t)nq * kmax * 4, cudaMemcpyDeviceToHost, st), "copy distances");
-    BF_CUDA(cudaMemcpyAsync(counts, o_c, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
+    const HostPiece down[3] = {{ids, o_ids, (size_t)nq * kmax * 4}, {dists, o_d, (size_t)nq * kmax * 4},
+                               {counts, o_c, (size_t)nq * 4}};
+    BF_CUDA(copy_to_host(h->pin_out, h->cfg.host_copy == 0, down, 3, st), "copy results");
+  } else {
+    BF_CUDA(cudaStreamSynchronize(st), "exact scan");
   }
-  BF_CUDA(cudaStreamSynchronize(st), "exact scan");
   if (stats) {
     stats[0] = 0;
     stats[1] = d.n;
@@ -1208,7 +1210,8 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
   const float* qin = queries;
   if (!dev_ptrs) {
     BF_CUDA(s->h_q.ensure((size_t)nq * dim * 4, false), "cudaMalloc(query staging)");
-    BF_CUDA(cudaMemcpyAsync(s->h_q.p, queries, (size_t)nq * dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
+    const HostPiece up{s->h_q.p, queries, (size_t)nq * dim * 4};
+    BF_CUDA(copy_to_device(h->pin_in, h->cfg.host_copy == 0, &up, 1, st), "copy queries");
     qin = s->h_q.as<float>();
   }
   BF_CUDA(s->q32.ensure((size_t)nq * dim * 4, false), "cudaMalloc");
@@ -1369,11 +1372,12 @@ extern "C" NMSG_API int nmsg_bruteforce_knn(nmsg_index* h, const float* queries,
       s->qn_hi.as<float>(), s->qn_lo.as<float>(), h->dev.ext_id, o_ids, o_d, o_c);
   BF_CUDA(cudaGetLastError(), "finish");
   if (!dev_ptrs) {
-    BF_CUDA(cudaMemcpyAsync(ids, o_ids, (size_t)nq * kmax * 4, cudaMemcpyDeviceToHost, st), "copy ids");
-    BF_CUDA(cudaMemcpyAsync(dists, o_d, (size_t)nq * kmax * 4, cudaMemcpyDeviceToHost, st), "copy distances");
-    BF_CUDA(cudaMemcpyAsync(counts, o_c, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
+    const HostPiece down[3] = {{ids, o_ids, (size_t)nq * kmax * 4}, {dists, o_d, (size_t)nq * kmax * 4},
+                               {counts, o_c, (size_t)nq * 4}};
+    BF_CUDA(copy_to_host(h->pin_out, h->cfg.host_copy == 0, down, 3, st), "copy results");
+  } else {
+    BF_CUDA(cudaStreamSynchronize(st), "brute-force results");
   }
-  BF_CUDA(cudaStreamSynchronize(st), "brute-force results");
   if (stats) {
     stats[0] = (int64_t)s_tiles * BN;  // sample rows (the last tile may be partial)
     stats[1] = max_collected;

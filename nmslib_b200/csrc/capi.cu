@@ -408,8 +408,10 @@ void nmsg_index_free(nmsg_index* h) {
     h->bf = nullptr;
     for (DevBuf* b : {&h->vecs, &h->norms, &h->l0, &h->up_off, &h->up_links, &h->ext_id, &h->visited, &h->epochs, &h->locks,
                       &h->old_heap, &h->counter, &h->status, &h->order, &h->kq, &h->efq, &h->q_stage,
-                      &h->ids_stage, &h->dists_stage, &h->counts_stage, &h->stats_stage})
+                      &h->ids_stage, &h->dists_stage, &h->counts_stage, &h->stats_stage, &h->entry})
       b->release();
+    h->pin_in.release();
+    h->pin_out.release();
   }
   delete h;
 }
@@ -442,15 +444,18 @@ int nmsg_set_query_params(nmsg_index* h, int ef, int algo) {
 
 int nmsg_last_device_status(const nmsg_index* h) { return h ? h->last_status : NMSG_ERR_BAD_ARG; }
 
+int nmsg_last_kernel_launches(const nmsg_index* h) { return h ? h->last_launches : NMSG_ERR_BAD_ARG; }
+
 int nmsg_set_launch_config(nmsg_index* h, const nmsg_launch_config* cfg) {
   if (!h) return fail(NMSG_ERR_BAD_ARG, "null index");
-  nmsg_launch_config c{0, 0, 0, 0, 0, 0, 0, 0};
+  nmsg_launch_config c{0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (cfg) {
     c = *cfg;
     if (c.plain_slots < 0) return fail(NMSG_ERR_BAD_ARG, "plain_slots must be >= 0");
     if (c.queries_per_warp < 0 || c.queries_per_warp > 4) return fail(NMSG_ERR_BAD_ARG, "queries_per_warp must be 0..4");
     if (c.row_copy < 0 || c.row_copy > 2) return fail(NMSG_ERR_BAD_ARG, "row_copy must be 0, 1 or 2");
     if (c.query_order != 0 && c.query_order != -1) return fail(NMSG_ERR_BAD_ARG, "query_order must be 0 or -1");
+    if (c.host_copy != 0 && c.host_copy != 1) return fail(NMSG_ERR_BAD_ARG, "host_copy must be 0 or 1");
     const int w = c.warps_per_block, r = c.rows_per_group, hl = c.visited_hash_log2, sr = c.stage_rows;
     if (!(w == 0 || w == 1 || w == 2 || w == 4)) return fail(NMSG_ERR_BAD_ARG, "warps_per_block must be 0, 1, 2 or 4");
     if (!(r == 0 || r == 1 || r == 2 || r == 4)) return fail(NMSG_ERR_BAD_ARG, "rows_per_group must be 0, 1, 2 or 4");
@@ -480,6 +485,7 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
   if (dev_ptrs && (k_per_q || ef_per_q))
     return fail(NMSG_ERR_BAD_ARG, "per-query k/ef arrays are host arrays; pass host buffers for mixed batches");
   std::lock_guard<std::mutex> lk(h->mu);
+  h->last_launches = 0;
   const int ef = h->ef, algo = h->algo;
   // per-query parameters and capacity of the shared-memory region
   int region = 1;
@@ -596,7 +602,9 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
     NMSG_CUDA(h->dists_stage.ensure(obytes, false), "cudaMalloc(distance staging)");
     NMSG_CUDA(h->counts_stage.ensure((size_t)nq * 4, false), "cudaMalloc(count staging)");
     if (stats) NMSG_CUDA(h->stats_stage.ensure((size_t)nq * 32, false), "cudaMalloc(stats staging)");
-    NMSG_CUDA(cudaMemcpyAsync(h->q_stage.p, queries_v, qbytes, cudaMemcpyHostToDevice, st), "copy queries");
+    HostPiece up[3];
+    int nup = 0;
+    up[nup++] = HostPiece{h->q_stage.p, queries_v, qbytes};
     if (u8)
       a.queries_u8 = h->q_stage.as<uint8_t>();
     else
@@ -607,12 +615,12 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
     a.stats = stats ? h->stats_stage.as<int64_t>() : nullptr;
     if (k_per_q) {
       NMSG_CUDA(h->kq.ensure((size_t)nq * 4, false), "cudaMalloc(k per query)");
-      NMSG_CUDA(cudaMemcpyAsync(h->kq.p, k_per_q, nq * 4, cudaMemcpyHostToDevice, st), "copy k");
+      up[nup++] = HostPiece{h->kq.p, k_per_q, (size_t)nq * 4};
       a.k_per_q = h->kq.as<int32_t>();
     }
     if (ef_per_q) {
       NMSG_CUDA(h->efq.ensure((size_t)nq * 4, false), "cudaMalloc(ef per query)");
-      NMSG_CUDA(cudaMemcpyAsync(h->efq.p, ef_per_q, nq * 4, cudaMemcpyHostToDevice, st), "copy ef");
+      up[nup++] = HostPiece{h->efq.p, ef_per_q, (size_t)nq * 4};
       a.ef_per_q = h->efq.as<int32_t>();
       // most expensive queries first, so the persistent warps finish together
       std::vector<int32_t> order(nq);
@@ -622,6 +630,7 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
       NMSG_CUDA(cudaMemcpy(h->order.p, order.data(), nq * 4, cudaMemcpyHostToDevice), "copy order");
       a.order = h->order.as<int32_t>();
     }
+    NMSG_CUDA(copy_to_device(h->pin_in, h->cfg.host_copy == 0, up, nup, st), "copy queries");
   }
   a.nbpad = plan.nbpad;
   // Split search: worth it once the batch outnumbers the resident warps (some warps then run
@@ -637,6 +646,8 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
     a.entry_order = e + 5 * nq;
     a.entry_range = reinterpret_cast<uint32_t*>(e + 6 * nq);
   }
+  // launch_search runs the descent, the order kernel and level 0 when the entry arrays are set
+  const int split_launches = (!plain && a.entry_node) ? 3 : 1;
   if (dev_ptrs && (flags & NMSG_CUDA_GRAPH)) {
     // Replay the captured launch when every argument is the same as last time; otherwise
     // capture (counter and status resets + kernel) into a new graph.
@@ -671,20 +682,22 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
       h->graph_shape[4] = wpb;
     }
     NMSG_CUDA(cudaGraphLaunch(h->graph_exec, st), "graph launch");
+    h->last_launches = split_launches;
     return NMSG_OK;
   }
   NMSG_CUDA(cudaMemsetAsync(a.work_counter, 0, 4, st), "reset counter");
   NMSG_CUDA(cudaMemsetAsync(a.status, 0, 4, st), "reset status");
   rc = launch_search(a, plain, gather, any_old, blocks, wpb, stream);
   if (rc != 0) return cuda_fail((cudaError_t)rc, "search kernel launch");
+  h->last_launches = split_launches;
   if (dev_ptrs) return NMSG_OK;
   int32_t dstatus = 0;
-  NMSG_CUDA(cudaMemcpyAsync(ids, a.ids, obytes, cudaMemcpyDeviceToHost, st), "copy ids");
-  NMSG_CUDA(cudaMemcpyAsync(dists_v, a.dists, obytes, cudaMemcpyDeviceToHost, st), "copy distances");
-  NMSG_CUDA(cudaMemcpyAsync(counts, a.counts, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
-  if (stats) NMSG_CUDA(cudaMemcpyAsync(stats, a.stats, nq * 32, cudaMemcpyDeviceToHost, st), "copy stats");
-  NMSG_CUDA(cudaMemcpyAsync(&dstatus, a.status, 4, cudaMemcpyDeviceToHost, st), "copy status");
-  NMSG_CUDA(cudaStreamSynchronize(st), "search");
+  const HostPiece down[5] = {{ids, a.ids, obytes},
+                             {dists_v, a.dists, obytes},
+                             {counts, a.counts, (size_t)nq * 4},
+                             {&dstatus, a.status, 4},
+                             {stats, a.stats, stats ? (size_t)nq * 32 : 0}};
+  NMSG_CUDA(copy_to_host(h->pin_out, h->cfg.host_copy == 0, down, stats ? 5 : 4, st), "copy results");
   h->last_status = dstatus;
   if (dstatus != 0) return fail(dstatus, "the search kernel reported a device-side error (status " + std::to_string(dstatus) + ")");
   return NMSG_OK;

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "engine.h"
+#include "host_stage.h"
 #include "../../include/nmslib_b200.h"
 
 namespace nmsg {
@@ -102,11 +103,13 @@ struct nmsg_index {
   nmsg::DevBuf visited, epochs, locks, old_heap, counter, status, order, kq, efq;
   nmsg::DevBuf entry;       // split lean search: entry nodes, distances, counts, key range, order
   nmsg::DevBuf q_stage, ids_stage, dists_stage, counts_stage, stats_stage;
+  nmsg::PinBuf pin_in, pin_out;  // page-locked staging of pageable host buffers
   int slots = 0;            // slots covered by visited/epochs/locks
   int64_t old_cap = 0;      // entries per slot in old_heap
   int64_t resident_bytes = 0;
   int last_status = NMSG_OK;
-  nmsg_launch_config cfg{0, 0, 0, 0, 0, 0, 0, 0};
+  int last_launches = 0;    // search kernels of the last batch call
+  nmsg_launch_config cfg{0, 0, 0, 0, 0, 0, 0, 0, 0};
   nmsg::BruteForceState* bf = nullptr;  // brute-force data, built on first use
   cudaGraphExec_t graph_exec = nullptr;  // last captured device-pointer search (NMSG_CUDA_GRAPH)
   cudaStream_t capture_stream = nullptr;

@@ -474,7 +474,7 @@ int insert_level0_on_device(Builder& b, const int32_t* nodes, int64_t count, int
   const int efc = b.efc;
   LaunchPlan plan;
   std::string perr;
-  const nmsg_launch_config cfg{0, 0, 0, 0, 0, 1, 0, -1};  // one construction search per warp, one pass
+  const nmsg_launch_config cfg{0, 0, 0, 0, 0, 1, 0, -1, 0};  // one construction search per warp, one pass
   int rc = plan_launch(d, cfg, efc, false, false, &plan, &perr);
   if (rc != NMSG_OK) {
     g_build_err = "device build: " + perr;

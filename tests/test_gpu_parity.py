@@ -434,3 +434,78 @@ def test_cuda_graph_replays_the_split_search():
         np.testing.assert_array_equal(ids.cpu().numpy(), want[0])
         np.testing.assert_array_equal(d.cpu().numpy().view(np.int32), want[1].view(np.int32))
         np.testing.assert_array_equal(c.cpu().numpy(), want[2])
+
+
+@pytest.mark.parametrize("rows", [1000, 2049, 12000])
+def test_host_copies_staged_and_direct(rows):
+    """Host-buffer batches of 512 KB and more travel through page-locked staging that host threads
+    fill in 1 MB chunks (host_copy 0, the default); host_copy 1 copies the caller's arrays
+    directly, and page-locked caller arrays are copied directly either way. Per-query k and
+    efSearch arrays travel with the queries. Every route returns the oracle's results."""
+    import torch
+
+    name = "c1_l2_d128"
+    q0 = load_golden(name)["queries"]
+    reps = -(-rows // len(q0))
+    base = np.arange(rows) % len(q0)
+    q = np.ascontiguousarray(np.tile(q0, (reps, 1))[:rows])
+    rng = np.random.default_rng(rows)
+    ks = rng.choice([1, 10, 32], size=rows).astype(np.int32)
+    efs = rng.choice([10, 64, 100], size=rows).astype(np.int32)
+    pinned = torch.empty(q.shape, dtype=torch.float32, pin_memory=True).numpy()
+    pinned[:] = q
+    idx = _gpu_index(name)
+    orc = _oracle(name)
+    want = {}
+    for kk in (1, 10, 32):
+        for ee in (10, 64, 100):
+            want[kk, ee] = orc.search(q0, k=kk, ef=ee, algo=ALGO_CODES["v1merge"])
+    try:
+        idx.setQueryTimeParams({"efSearch": 64, "algoType": "v1merge"})
+        for host_copy in (0, 1):
+            idx.setLaunchConfig(host_copy=host_copy)
+            for arr in (q, pinned):
+                ids, d, cnt, st = idx.knnQueryBatchArrays(arr, 10, stats=True)
+                oi, od, oc, ost = want[10, 64]
+                np.testing.assert_array_equal(cnt, oc[base])
+                np.testing.assert_array_equal(ids, oi[base])
+                np.testing.assert_array_equal(d.view(np.int32), od[base].view(np.int32))
+                np.testing.assert_array_equal(st, ost[base])
+                ids, d, cnt = idx.knnQueryBatchArrays(arr, ks, ef=efs)
+                for (kk, ee), (oi, od, oc, _) in want.items():
+                    m = (ks == kk) & (efs == ee)
+                    b = base[m]
+                    np.testing.assert_array_equal(cnt[m], oc[b])
+                    live = np.arange(kk)[None, :] < oc[b][:, None]
+                    np.testing.assert_array_equal(np.where(live, ids[m, :kk], -1), np.where(live, oi[b], -1))
+                    np.testing.assert_array_equal(np.where(live, d[m, :kk].view(np.int32), 0),
+                                                  np.where(live, od[b].view(np.int32), 0))
+    finally:
+        idx.setLaunchConfig()
+
+
+def test_kernel_launch_count_of_the_last_batch():
+    """nmsg_last_kernel_launches: one launch for a batch that fits the resident warps, for the
+    one-query-per-block kernel and with query_order -1; three (descent, entry order, level 0) for a
+    larger V1Merge batch."""
+    from nmslib_b200 import _capi
+
+    lib = _capi.load()
+    idx = _gpu_index("c1_l2_d128")
+    q = load_golden("c1_l2_d128")["queries"]
+    big = np.ascontiguousarray(np.tile(q, (-(-12000 // len(q)), 1)))
+    idx.setQueryTimeParams({"efSearch": 64, "algoType": "v1merge"})
+    idx.knnQueryBatchArrays(q[:100], 10)
+    assert lib.nmsg_last_kernel_launches(idx._h) == 1
+    idx.knnQueryBatchArrays(q[:100], 10, plain=True)
+    assert lib.nmsg_last_kernel_launches(idx._h) == 1
+    idx.knnQueryBatchArrays(big, 10)
+    assert lib.nmsg_last_kernel_launches(idx._h) == 3
+    idx.setLaunchConfig(query_order=-1)
+    try:
+        idx.knnQueryBatchArrays(big, 10)
+        assert lib.nmsg_last_kernel_launches(idx._h) == 1
+    finally:
+        idx.setLaunchConfig()
+    idx.knnQueryBatchArrays(q[:0], 10)
+    assert lib.nmsg_last_kernel_launches(idx._h) == 0
