@@ -292,8 +292,10 @@ NMSG_API int nmsg_last_device_status(const nmsg_index* index);
 
 /* Search kernels the last nmsg_knn_batch / nmsg_knn_batch_u8 call on this handle launched (under
  * NMSG_CUDA_GRAPH: launched by the graph it replayed): 1 for one pass, 3 for a batch that runs the
- * upper-level descent, the entry ordering and level 0 as separate passes; 0 when it launched none
- * (an empty batch or index, or a call that failed before launching). */
+ * upper-level descent, the entry ordering and level 0 as separate passes, 4 when that descent runs
+ * in two halves (pageable host queries copied in two parts, the first half's descents overlapping
+ * the second half's copy); 0 when it launched none (an empty batch or index, or a call that failed
+ * before launching). */
 NMSG_API int nmsg_last_kernel_launches(const nmsg_index* index);
 
 NMSG_API const char* nmsg_last_error(void);

@@ -404,6 +404,12 @@ void nmsg_index_free(nmsg_index* h) {
     DeviceGuard g(h->device);
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
+    if (h->copy_stream) {
+      cudaStreamSynchronize(h->copy_stream);
+      cudaStreamDestroy(h->copy_stream);
+    }
+    for (cudaEvent_t ev : h->part_ev)
+      if (ev) cudaEventDestroy(ev);
     destroy_bruteforce(h->bf);
     h->bf = nullptr;
     for (DevBuf* b : {&h->vecs, &h->norms, &h->l0, &h->up_off, &h->up_links, &h->ext_id, &h->visited, &h->epochs, &h->locks,
@@ -585,6 +591,14 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
   a.work_counter = h->counter.as<int32_t>();
   a.status = h->status.as<int32_t>();
 
+  // Split search: worth it once the batch outnumbers the resident warps (some warps then run
+  // several queries, and which queries start last decides when the batch ends). V1Merge batches of
+  // one efSearch on the one-query-per-warp kernels.
+  const bool split =
+      (plan.lean || (plan.ctx == 1 && !any_old)) && !plain && !ef_per_q && nq > slots && h->cfg.query_order != -1;
+  QueryParts parts;
+  bool use_parts = false;
+
   // inputs / outputs
   const size_t qbytes = (size_t)nq * dim * (u8 ? 1 : 4), obytes = (size_t)nq * kmax * 4;
   if (dev_ptrs) {
@@ -630,13 +644,27 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
       NMSG_CUDA(cudaMemcpy(h->order.p, order.data(), nq * 4, cudaMemcpyHostToDevice), "copy order");
       a.order = h->order.as<int32_t>();
     }
-    NMSG_CUDA(copy_to_device(h->pin_in, h->cfg.host_copy == 0, up, nup, st), "copy queries");
+    if (split && plan.lean && use_staging(h->cfg.host_copy == 0, up, nup, true)) {
+      // Two halves on the handle's copy stream: the first half's descents start while the second
+      // half is still being copied.
+      if (!h->copy_stream) {
+        NMSG_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking), "copy stream");
+        for (cudaEvent_t& ev : h->part_ev) NMSG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+      }
+      NMSG_CUDA(cudaEventRecord(h->part_ev[2], st), "record");  // after the caller's earlier work on st
+      NMSG_CUDA(cudaStreamWaitEvent(h->copy_stream, h->part_ev[2], 0), "wait");
+      parts.first = nq / 2;
+      parts.ready[0] = h->part_ev[0];
+      parts.ready[1] = h->part_ev[1];
+      NMSG_CUDA(upload_staged_parts(h->pin_in, up, nup, (size_t)parts.first * dim * 4, h->copy_stream, h->part_ev),
+                "copy queries");
+      use_parts = true;
+    } else {
+      NMSG_CUDA(copy_to_device(h->pin_in, h->cfg.host_copy == 0, up, nup, st), "copy queries");
+    }
   }
   a.nbpad = plan.nbpad;
-  // Split search: worth it once the batch outnumbers the resident warps (some warps then run
-  // several queries, and which queries start last decides when the batch ends). V1Merge batches of
-  // one efSearch on the one-query-per-warp kernels.
-  if ((plan.lean || (plan.ctx == 1 && !any_old)) && !plain && !a.order && nq > slots && h->cfg.query_order != -1) {
+  if (split) {
     const size_t words = (size_t)nq * 6 + 4;  // node, distance, 3 counts, order; range
     NMSG_CUDA(h->entry.ensure(words * 4, false), "cudaMalloc(level-0 entries)");
     int32_t* e = h->entry.as<int32_t>();
@@ -687,9 +715,9 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
   }
   NMSG_CUDA(cudaMemsetAsync(a.work_counter, 0, 4, st), "reset counter");
   NMSG_CUDA(cudaMemsetAsync(a.status, 0, 4, st), "reset status");
-  rc = launch_search(a, plain, gather, any_old, blocks, wpb, stream);
+  rc = launch_search(a, plain, gather, any_old, blocks, wpb, stream, use_parts ? &parts : nullptr);
   if (rc != 0) return cuda_fail((cudaError_t)rc, "search kernel launch");
-  h->last_launches = split_launches;
+  h->last_launches = split_launches + (use_parts ? 1 : 0);
   if (dev_ptrs) return NMSG_OK;
   int32_t dstatus = 0;
   const HostPiece down[5] = {{ids, a.ids, obytes},

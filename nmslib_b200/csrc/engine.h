@@ -5,6 +5,7 @@
 #include <string>
 #include <vector>
 
+#include <driver_types.h>
 #include <vector_types.h>
 
 #ifdef __CUDACC__
@@ -139,6 +140,7 @@ struct SearchArgs {
   int32_t* entry_stats = nullptr;   // [nq][3]
   uint32_t* entry_range = nullptr;  // [2]: smallest and largest ordered key
   int32_t* entry_order = nullptr;   // [nq]: the level-0 pass's work order (largest entry distance first)
+  int64_t q_base = 0;               // a lean descent pass over part of the batch: queries q_base + [0, nq)
   int32_t* slot_locks = nullptr;    // [num_slots] (one-query-per-block kernel only)
   int num_slots = 0;
   uint2* old_heap = nullptr;        // [num_slots][old_heap_cap] SearchOld candidate heaps
@@ -183,8 +185,14 @@ NMSG_HD inline int bulk_row_bytes(const DevIndex& ix) { return ((ix.dim * 4 + 15
 // vector rows are fetched: 0 = asynchronous copies into shared memory (stage_rows per round),
 // 1/2/4 = registers, that many rows per 8-lane group. `with_old` includes the SearchOld path.
 // Return a cudaError_t value.
+// Queries of a split lean search that reach the device in two parts (host uploads on another
+// stream): the descent pass of queries [0, first) waits for ready[0], that of the rest for ready[1].
+struct QueryParts {
+  int64_t first = 0;
+  cudaEvent_t ready[2] = {nullptr, nullptr};
+};
 int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, int blocks, int warps_per_block,
-                  void* stream);
+                  void* stream, const QueryParts* parts = nullptr);
 
 // Opt-in dynamic shared memory of the current device (227 KB on B200).
 constexpr int kMaxDynamicSmem = 227 * 1024;

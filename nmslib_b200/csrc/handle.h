@@ -113,6 +113,8 @@ struct nmsg_index {
   nmsg::BruteForceState* bf = nullptr;  // brute-force data, built on first use
   cudaGraphExec_t graph_exec = nullptr;  // last captured device-pointer search (NMSG_CUDA_GRAPH)
   cudaStream_t capture_stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // two-part query uploads of split searches
+  cudaEvent_t part_ev[3] = {nullptr, nullptr, nullptr};  // first half copied, all copied, start
   nmsg::SearchArgs graph_args{};
   int graph_shape[5] = {0, 0, 0, 0, 0};
   std::mutex mu;

@@ -2080,7 +2080,7 @@ __global__ void __launch_bounds__(1024) order_by_entry_kernel(const float* __res
 }  // namespace
 
 int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, int blocks, int warps_per_block,
-                  void* stream) {
+                  void* stream, const QueryParts* parts) {
   Kern kern = a.lean ? lean_kernel_for(a.ix) : kernel_for(plain, gather, with_old, a.ctx_per_warp, multi_list_chunks(a.ix));
   if (!kern) return (int)cudaErrorInvalidDeviceFunction;
   const int smem = a.warp_smem * (plain ? 1 : warps_per_block);
@@ -2097,7 +2097,25 @@ int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, in
     if (e == cudaSuccess) e = cudaMemsetAsync(a.entry_range, 0xff, 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.entry_range + 1, 0, 4, st);
     if (e != cudaSuccess) return (int)e;
-    kern<<<blocks, 32 * warps_per_block, smem, st>>>(d);
+    if (parts && a.lean && parts->first > 0 && parts->first < a.nq) {
+      // the first part's descents run while the rest of the queries are still being copied
+      e = cudaStreamWaitEvent(st, parts->ready[0], 0);
+      if (e != cudaSuccess) return (int)e;
+      d.nq = parts->first;
+      kern<<<blocks, 32 * warps_per_block, smem, st>>>(d);
+      e = cudaMemsetAsync(a.work_counter, 0, 4, st);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(st, parts->ready[1], 0);
+      if (e != cudaSuccess) return (int)e;
+      d.q_base = parts->first;
+      d.nq = a.nq - parts->first;
+      kern<<<blocks, 32 * warps_per_block, smem, st>>>(d);
+    } else {
+      if (parts) {
+        e = cudaStreamWaitEvent(st, parts->ready[1], 0);
+        if (e != cudaSuccess) return (int)e;
+      }
+      kern<<<blocks, 32 * warps_per_block, smem, st>>>(d);
+    }
     order_by_entry_kernel<<<1, 1024, 0, st>>>(a.entry_dist, a.nq, a.entry_range, a.entry_order);
     e = cudaMemsetAsync(a.work_counter, 0, 4, st);
     if (e != cudaSuccess) return (int)e;
@@ -2106,6 +2124,10 @@ int launch_search(const SearchArgs& a, bool plain, int gather, bool with_old, in
     l.order = a.entry_order;
     kern<<<blocks, 32 * warps_per_block, smem, st>>>(l);
     return (int)cudaGetLastError();
+  }
+  if (parts) {
+    const cudaError_t e = cudaStreamWaitEvent((cudaStream_t)stream, parts->ready[1], 0);
+    if (e != cudaSuccess) return (int)e;
   }
   if (plain)
     kern<<<(unsigned)a.nq, 32, smem, (cudaStream_t)stream>>>(a);

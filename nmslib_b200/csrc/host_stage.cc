@@ -313,9 +313,42 @@ size_t total_bytes(const HostPiece* pieces, int n) {
 
 }  // namespace
 
+bool use_staging(bool stage, const HostPiece* pieces, int n, bool host_src) {
+  return stage && n > 0 && total_bytes(pieces, n) >= kStageMinBytes &&
+         pageable(host_src ? pieces[0].src : pieces[0].dst, pieces[0].bytes);
+}
+
+cudaError_t upload_staged_parts(PinBuf& pin, const HostPiece* pieces, int n, size_t first_bytes, cudaStream_t cs,
+                                cudaEvent_t ready[2]) {
+  size_t need = 0;
+  for (int i = 0; i < n; ++i) need += pin_round(pieces[i].bytes);
+  cudaError_t e = pin.ensure(need);
+  if (e != cudaSuccess) return e;
+  std::vector<HostPiece> fill(n);
+  size_t off = 0;
+  for (int i = 0; i < n; ++i) {
+    fill[i] = HostPiece{pin.as<char>() + off, pieces[i].src, pieces[i].bytes};
+    off += pin_round(pieces[i].bytes);
+  }
+  host_copy(fill.data(), n);
+  first_bytes = std::min(first_bytes, pieces[0].bytes);
+  auto dma = [&](void* dst, const void* src, size_t bytes) {
+    if (!bytes) return cudaSuccess;
+    cudaError_t r = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, cs);
+    return r == cudaSuccess ? pin.mark(cs) : r;
+  };
+  e = dma(pieces[0].dst, fill[0].dst, first_bytes);
+  if (e == cudaSuccess) e = cudaEventRecord(ready[0], cs);
+  if (e == cudaSuccess)
+    e = dma(static_cast<char*>(pieces[0].dst) + first_bytes, static_cast<const char*>(fill[0].dst) + first_bytes,
+            pieces[0].bytes - first_bytes);
+  for (int i = 1; i < n && e == cudaSuccess; ++i) e = dma(pieces[i].dst, fill[i].dst, pieces[i].bytes);
+  if (e == cudaSuccess) e = cudaEventRecord(ready[1], cs);
+  return e;
+}
+
 cudaError_t copy_to_device(PinBuf& pin, bool stage, const HostPiece* pieces, int n, cudaStream_t st) {
-  if (stage && total_bytes(pieces, n) >= kStageMinBytes && pageable(pieces[0].src, pieces[0].bytes))
-    return upload_staged(pin, pieces, n, st);
+  if (use_staging(stage, pieces, n, true)) return upload_staged(pin, pieces, n, st);
   for (int i = 0; i < n; ++i) {
     if (!pieces[i].bytes) continue;
     const cudaError_t e = cudaMemcpyAsync(pieces[i].dst, pieces[i].src, pieces[i].bytes, cudaMemcpyHostToDevice, st);
@@ -325,8 +358,7 @@ cudaError_t copy_to_device(PinBuf& pin, bool stage, const HostPiece* pieces, int
 }
 
 cudaError_t copy_to_host(PinBuf& pin, bool stage, const HostPiece* pieces, int n, cudaStream_t st) {
-  if (stage && total_bytes(pieces, n) >= kStageMinBytes && pageable(pieces[0].dst, pieces[0].bytes))
-    return download_staged(pin, pieces, n, st);
+  if (use_staging(stage, pieces, n, false)) return download_staged(pin, pieces, n, st);
   for (int i = 0; i < n; ++i) {
     if (!pieces[i].bytes) continue;
     const cudaError_t e = cudaMemcpyAsync(pieces[i].dst, pieces[i].src, pieces[i].bytes, cudaMemcpyDeviceToHost, st);

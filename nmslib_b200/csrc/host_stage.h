@@ -58,13 +58,22 @@ bool is_page_locked(const void* p);
 // Batches whose host buffers total fewer bytes than this are copied directly.
 constexpr size_t kStageMinBytes = 512 * 1024;
 
+// Whether copies of these pieces go through staging: `stage` allows it, they total kStageMinBytes
+// or more, and the first piece's host buffer (`host_src`: its source, else its destination) is
+// pageable.
+bool use_staging(bool stage, const HostPiece* pieces, int n, bool host_src);
+
+// upload_staged in two parts on `cs`: one fill of every piece, then the DMA of the first
+// `first_bytes` of piece 0 followed by ready[0], then the DMAs of the rest followed by ready[1].
+cudaError_t upload_staged_parts(PinBuf& pin, const HostPiece* pieces, int n, size_t first_bytes, cudaStream_t cs,
+                                cudaEvent_t ready[2]);
+
 // Queues on `st` the copies of a call's inputs (src: host memory, dst: device memory): through
-// upload_staged when `stage` allows it, they total kStageMinBytes or more and the first piece's
-// host buffer is pageable; otherwise directly.
+// upload_staged when use_staging says so; otherwise directly.
 cudaError_t copy_to_device(PinBuf& pin, bool stage, const HostPiece* pieces, int n, cudaStream_t st);
 
 // Copies a call's results back (src: device memory, dst: host memory) and waits for `st`: through
-// download_staged on the same conditions, otherwise directly.
+// download_staged when use_staging says so, otherwise directly.
 cudaError_t copy_to_host(PinBuf& pin, bool stage, const HostPiece* pieces, int n, cudaStream_t st);
 
 // Queues on `st` the copies of every piece (src: host memory, dst: device memory) through `pin`:

@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(128, 8) search_lean_kernel(SearchArgs a) {
     if (lane == 0) item = atomicAdd(a.work_counter, 1);
     item = __shfl_sync(kFull, item, 0);
     if (item >= a.nq) break;
-    const int64_t qi = a.order ? a.order[item] : item;
+    const int64_t qi = a.order ? a.order[item] : a.q_base + item;
     // next epoch of this slot's visited bytes; cleared when the byte wraps (hnsw.h:582-589). The
     // descent pass of a split search touches no visited set.
     int ep = 0;

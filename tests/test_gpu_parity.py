@@ -487,7 +487,8 @@ def test_host_copies_staged_and_direct(rows):
 def test_kernel_launch_count_of_the_last_batch():
     """nmsg_last_kernel_launches: one launch for a batch that fits the resident warps, for the
     one-query-per-block kernel and with query_order -1; three (descent, entry order, level 0) for a
-    larger V1Merge batch."""
+    larger V1Merge batch copied directly, four when its pageable queries travel in two halves (the
+    descent split in two)."""
     from nmslib_b200 import _capi
 
     lib = _capi.load()
@@ -500,7 +501,13 @@ def test_kernel_launch_count_of_the_last_batch():
     idx.knnQueryBatchArrays(q[:100], 10, plain=True)
     assert lib.nmsg_last_kernel_launches(idx._h) == 1
     idx.knnQueryBatchArrays(big, 10)
-    assert lib.nmsg_last_kernel_launches(idx._h) == 3
+    assert lib.nmsg_last_kernel_launches(idx._h) == 4
+    idx.setLaunchConfig(host_copy=1)
+    try:
+        idx.knnQueryBatchArrays(big, 10)
+        assert lib.nmsg_last_kernel_launches(idx._h) == 3
+    finally:
+        idx.setLaunchConfig()
     idx.setLaunchConfig(query_order=-1)
     try:
         idx.knnQueryBatchArrays(big, 10)
