@@ -516,3 +516,38 @@ def test_kernel_launch_count_of_the_last_batch():
         idx.setLaunchConfig()
     idx.knnQueryBatchArrays(q[:0], 10)
     assert lib.nmsg_last_kernel_launches(idx._h) == 0
+
+
+def test_host_buffers_on_a_caller_stream():
+    """nmsg_knn_batch with pageable host buffers on the caller's own stream, which still has work
+    queued: a batch larger than the resident warps copies its queries in two halves on the
+    handle's copy stream after that work, and returns the results of the default-stream call."""
+    import ctypes
+
+    import torch
+
+    from nmslib_b200 import _capi
+
+    lib = _capi.load()
+    idx = _gpu_index("c1_l2_d128")
+    q0 = load_golden("c1_l2_d128")["queries"]
+    q = np.ascontiguousarray(np.tile(q0, (-(-12000 // len(q0)), 1)))
+    nq, dim = q.shape
+    idx.setQueryTimeParams({"efSearch": 64, "algoType": "v1merge"})
+    want = idx.knnQueryBatchArrays(q, 10)
+    s = torch.cuda.Stream()
+    busy = torch.empty(1 << 28, dtype=torch.uint8, device="cuda")
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    for _ in range(2):
+        with torch.cuda.stream(s):
+            busy.fill_(7)  # earlier work on the caller's stream
+        ids = np.full((nq, 10), -7, np.int32)
+        d = np.zeros((nq, 10), np.float32)
+        c = np.zeros(nq, np.int32)
+        rc = lib.nmsg_knn_batch(idx._h, ptr(q), nq, dim, 10, None, None, 10, ptr(ids), ptr(d), ptr(c), None, 0,
+                                s.cuda_stream)
+        assert rc == 0, _capi.last_error()
+        assert lib.nmsg_last_kernel_launches(idx._h) == 4
+        np.testing.assert_array_equal(c, want[2])
+        np.testing.assert_array_equal(ids, want[0])
+        np.testing.assert_array_equal(d.view(np.int32), want[1].view(np.int32))
