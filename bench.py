@@ -248,7 +248,7 @@ class ClockSampler:
     """nvidia-smi clock/throttle samples every 100 ms while the timed region runs."""
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_power_cap,clocks.mem")
     NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device):
@@ -284,11 +284,12 @@ class ClockSampler:
         num = lambda v: float(v) if v.replace(".", "", 1).isdigit() else None  # noqa: E731
         sm = [num(r[0]) for r in rows if r and num(r[0]) is not None]
         mx = [num(r[1]) for r in rows if len(r) > 1 and num(r[1]) is not None]
+        mem = [num(r[7]) for r in rows if len(r) > 7 and num(r[7]) is not None]
         reasons = sorted({self.NAMES[i] for r in rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "mem_mhz": statistics.median(mem) if mem else None, "reasons": reasons, "samples": len(rows)}
 
 
 # ------------------------------------------------------------------ ncu traffic record
