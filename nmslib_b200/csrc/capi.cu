@@ -644,9 +644,11 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
       NMSG_CUDA(cudaMemcpy(h->order.p, order.data(), nq * 4, cudaMemcpyHostToDevice), "copy order");
       a.order = h->order.as<int32_t>();
     }
-    if (split && plan.lean && use_staging(h->cfg.host_copy == 0, up, nup, true)) {
+    const bool staged = use_staging(h->cfg.host_copy == 0, up, nup, true);
+    const bool locked = !staged && h->cfg.host_copy == 0 && host_range_page_locked(up[0].src, up[0].bytes);
+    if (split && plan.lean && (staged || locked)) {
       // Two halves on the handle's copy stream: the first half's descents start while the second
-      // half is still being copied.
+      // half is still being copied (pageable queries through staging, page-locked ones directly).
       if (!h->copy_stream) {
         NMSG_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking), "copy stream");
         for (cudaEvent_t& ev : h->part_ev) NMSG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
@@ -656,8 +658,12 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
       parts.first = nq / 2;
       parts.ready[0] = h->part_ev[0];
       parts.ready[1] = h->part_ev[1];
-      NMSG_CUDA(upload_staged_parts(h->pin_in, up, nup, (size_t)parts.first * dim * 4, h->copy_stream, h->part_ev),
-                "copy queries");
+      if (staged)
+        NMSG_CUDA(upload_staged_parts(h->pin_in, up, nup, (size_t)parts.first * dim * 4, h->copy_stream, h->part_ev),
+                  "copy queries");
+      else
+        NMSG_CUDA(upload_parts_direct(up, nup, (size_t)parts.first * dim * 4, h->copy_stream, h->part_ev),
+                  "copy queries");
       use_parts = true;
     } else {
       NMSG_CUDA(copy_to_device(h->pin_in, h->cfg.host_copy == 0, up, nup, st), "copy queries");

@@ -347,6 +347,24 @@ cudaError_t upload_staged_parts(PinBuf& pin, const HostPiece* pieces, int n, siz
   return e;
 }
 
+cudaError_t upload_parts_direct(const HostPiece* pieces, int n, size_t first_bytes, cudaStream_t cs,
+                                cudaEvent_t ready[2]) {
+  first_bytes = std::min(first_bytes, pieces[0].bytes);
+  auto dma = [&](void* dst, const void* src, size_t bytes) {
+    return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, cs) : cudaSuccess;
+  };
+  cudaError_t e = dma(pieces[0].dst, pieces[0].src, first_bytes);
+  if (e == cudaSuccess) e = cudaEventRecord(ready[0], cs);
+  if (e == cudaSuccess)
+    e = dma(static_cast<char*>(pieces[0].dst) + first_bytes, static_cast<const char*>(pieces[0].src) + first_bytes,
+            pieces[0].bytes - first_bytes);
+  for (int i = 1; i < n && e == cudaSuccess; ++i) e = dma(pieces[i].dst, pieces[i].src, pieces[i].bytes);
+  if (e == cudaSuccess) e = cudaEventRecord(ready[1], cs);
+  return e;
+}
+
+bool host_range_page_locked(const void* p, size_t bytes) { return bytes && !pageable(p, bytes); }
+
 cudaError_t copy_to_device(PinBuf& pin, bool stage, const HostPiece* pieces, int n, cudaStream_t st) {
   if (use_staging(stage, pieces, n, true)) return upload_staged(pin, pieces, n, st);
   for (int i = 0; i < n; ++i) {

@@ -68,6 +68,15 @@ bool use_staging(bool stage, const HostPiece* pieces, int n, bool host_src);
 cudaError_t upload_staged_parts(PinBuf& pin, const HostPiece* pieces, int n, size_t first_bytes, cudaStream_t cs,
                                 cudaEvent_t ready[2]);
 
+// The copies of upload_staged_parts straight from the caller's buffers (page-locked ones, which
+// need no staging): the first `first_bytes` of piece 0 followed by ready[0], then the rest followed
+// by ready[1], on `cs`.
+cudaError_t upload_parts_direct(const HostPiece* pieces, int n, size_t first_bytes, cudaStream_t cs,
+                                cudaEvent_t ready[2]);
+
+// True when the whole host range is page-locked memory (both of its ends, see is_page_locked).
+bool host_range_page_locked(const void* p, size_t bytes);
+
 // Queues on `st` the copies of a call's inputs (src: host memory, dst: device memory): through
 // upload_staged when use_staging says so; otherwise directly.
 cudaError_t copy_to_device(PinBuf& pin, bool stage, const HostPiece* pieces, int n, cudaStream_t st);

@@ -487,8 +487,8 @@ def test_host_copies_staged_and_direct(rows):
 def test_kernel_launch_count_of_the_last_batch():
     """nmsg_last_kernel_launches: one launch for a batch that fits the resident warps, for the
     one-query-per-block kernel and with query_order -1; three (descent, entry order, level 0) for a
-    larger V1Merge batch copied directly, four when its pageable queries travel in two halves (the
-    descent split in two)."""
+    larger V1Merge batch copied directly, four when its queries travel in two halves (pageable ones
+    through staging, page-locked ones directly; the descent split in two)."""
     from nmslib_b200 import _capi
 
     lib = _capi.load()
@@ -502,6 +502,15 @@ def test_kernel_launch_count_of_the_last_batch():
     assert lib.nmsg_last_kernel_launches(idx._h) == 1
     idx.knnQueryBatchArrays(big, 10)
     assert lib.nmsg_last_kernel_launches(idx._h) == 4
+    import torch
+
+    pinned = torch.empty(big.shape, dtype=torch.float32, pin_memory=True).numpy()
+    pinned[:] = big
+    got = idx.knnQueryBatchArrays(pinned, 10)  # page-locked: two halves copied directly
+    assert lib.nmsg_last_kernel_launches(idx._h) == 4
+    want = idx.knnQueryBatchArrays(big, 10)
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)
     idx.setLaunchConfig(host_copy=1)
     try:
         idx.knnQueryBatchArrays(big, 10)
