@@ -644,7 +644,7 @@ int knn_batch_impl(nmsg_index* h, const void* queries_v, bool u8, int64_t nq, in
       NMSG_CUDA(cudaMemcpy(h->order.p, order.data(), nq * 4, cudaMemcpyHostToDevice), "copy order");
       a.order = h->order.as<int32_t>();
     }
-    const bool staged = use_staging(h->cfg.host_copy == 0, up, nup, true);
+    const bool staged = use_staging(h->pin_in, h->cfg.host_copy == 0, up, nup, true);
     const bool locked = !staged && h->cfg.host_copy == 0 && host_range_page_locked(up[0].src, up[0].bytes);
     if (split && plan.lean && (staged || locked)) {
       // Two halves on the handle's copy stream: the first half's descents start while the second

@@ -313,9 +313,17 @@ size_t total_bytes(const HostPiece* pieces, int n) {
 
 }  // namespace
 
-bool use_staging(bool stage, const HostPiece* pieces, int n, bool host_src) {
-  return stage && n > 0 && total_bytes(pieces, n) >= kStageMinBytes &&
-         pageable(host_src ? pieces[0].src : pieces[0].dst, pieces[0].bytes);
+bool use_staging(PinBuf& pin, bool stage, const HostPiece* pieces, int n, bool host_src) {
+  if (!(stage && n > 0 && total_bytes(pieces, n) >= kStageMinBytes &&
+        pageable(host_src ? pieces[0].src : pieces[0].dst, pieces[0].bytes)))
+    return false;
+  size_t need = 0;
+  for (int i = 0; i < n; ++i) need += pin_round(pieces[i].bytes);
+  if (pin.ensure(need) != cudaSuccess) {
+    cudaGetLastError();  // no page-locked memory: copy directly
+    return false;
+  }
+  return true;
 }
 
 cudaError_t upload_staged_parts(PinBuf& pin, const HostPiece* pieces, int n, size_t first_bytes, cudaStream_t cs,
@@ -366,7 +374,7 @@ cudaError_t upload_parts_direct(const HostPiece* pieces, int n, size_t first_byt
 bool host_range_page_locked(const void* p, size_t bytes) { return bytes && !pageable(p, bytes); }
 
 cudaError_t copy_to_device(PinBuf& pin, bool stage, const HostPiece* pieces, int n, cudaStream_t st) {
-  if (use_staging(stage, pieces, n, true)) return upload_staged(pin, pieces, n, st);
+  if (use_staging(pin, stage, pieces, n, true)) return upload_staged(pin, pieces, n, st);
   for (int i = 0; i < n; ++i) {
     if (!pieces[i].bytes) continue;
     const cudaError_t e = cudaMemcpyAsync(pieces[i].dst, pieces[i].src, pieces[i].bytes, cudaMemcpyHostToDevice, st);
@@ -376,7 +384,7 @@ cudaError_t copy_to_device(PinBuf& pin, bool stage, const HostPiece* pieces, int
 }
 
 cudaError_t copy_to_host(PinBuf& pin, bool stage, const HostPiece* pieces, int n, cudaStream_t st) {
-  if (use_staging(stage, pieces, n, false)) return download_staged(pin, pieces, n, st);
+  if (use_staging(pin, stage, pieces, n, false)) return download_staged(pin, pieces, n, st);
   for (int i = 0; i < n; ++i) {
     if (!pieces[i].bytes) continue;
     const cudaError_t e = cudaMemcpyAsync(pieces[i].dst, pieces[i].src, pieces[i].bytes, cudaMemcpyDeviceToHost, st);

@@ -58,10 +58,11 @@ bool is_page_locked(const void* p);
 // Batches whose host buffers total fewer bytes than this are copied directly.
 constexpr size_t kStageMinBytes = 512 * 1024;
 
-// Whether copies of these pieces go through staging: `stage` allows it, they total kStageMinBytes
-// or more, and the first piece's host buffer (`host_src`: its source, else its destination) is
-// pageable.
-bool use_staging(bool stage, const HostPiece* pieces, int n, bool host_src);
+// Whether copies of these pieces go through staging in `pin`: `stage` allows it, they total
+// kStageMinBytes or more, the first piece's host buffer (`host_src`: its source, else its
+// destination) is pageable, and `pin` holds (or could grow to) room for them. When page-locked
+// memory cannot be had, the copies go directly instead.
+bool use_staging(PinBuf& pin, bool stage, const HostPiece* pieces, int n, bool host_src);
 
 // upload_staged in two parts on `cs`: one fill of every piece, then the DMA of the first
 // `first_bytes` of piece 0 followed by ready[0], then the DMAs of the rest followed by ready[1].
